@@ -1,0 +1,196 @@
+// C entry points onto CarpetLib's own grid-transfer operators, compiled
+// unchanged from the reference sources by oracle/Makefile against the
+// stand-in headers in oracle/shim/.  TEST INFRASTRUCTURE: only the tests,
+// the smoke check and the CPU baseline of bench.py load the resulting
+// oracle/_ref/libcarpetref*.so; the product never does.
+//
+// Boxes are passed as int[9] = {lower[3], upper[3], stride[3]}, the layout
+// CarpetLib itself hands to its Fortran operators (CarpetLib/src/data.cc:
+// 212-214 reinterpret_casts an ibbox3 to int[3][3]).  Every entry point
+// returns 0 on success and 1 when the operator raised a Cactus error; the
+// message is then available from cgxref_last_error().
+#include <cstring>
+#include <exception>
+#include <string>
+
+#include "cctk.h"
+#include "gdata.hh"
+#include "operator_prototypes_3d.hh"
+
+using namespace CarpetLib;
+
+extern "C" int cgx_shim_use_openmp;
+
+namespace {
+thread_local std::string last_error;
+
+ivect3 iv(const int *p) { return ivect3(p[0], p[1], p[2]); }
+ibbox3 ib(const int *p) {
+  return ibbox3(ivect3(p[0], p[1], p[2]), ivect3(p[3], p[4], p[5]),
+                ivect3(p[6], p[7], p[8]));
+}
+
+typedef void (*op_t)(double const *, ivect3 const &, ivect3 const &, double *,
+                     ivect3 const &, ivect3 const &, ibbox3 const &,
+                     ibbox3 const &, ibbox3 const &, ibbox3 const &, void *);
+
+// The OpenMP split of CarpetLib/src/data.cc:56-93 (call_operator): each
+// thread takes a slab of the destination region along its longest axis.
+// The operators are pointwise, so the split never changes a result.
+void call_operator(op_t op, double const *src, ivect3 const &srcpadext,
+                   ivect3 const &srcext, double *dst, ivect3 const &dstpadext,
+                   ivect3 const &dstext, ibbox3 const &srcbbox,
+                   ibbox3 const &dstbbox, ibbox3 const &srcregbbox,
+                   ibbox3 const &dstregbbox) {
+  if (!cgx_shim_use_openmp) {
+    op(src, srcpadext, srcext, dst, dstpadext, dstext, srcbbox, dstbbox,
+       srcregbbox, dstregbbox, nullptr);
+    return;
+  }
+  std::string err;
+#pragma omp parallel
+  {
+    int const nthreads = omp_get_num_threads();
+    int const me = omp_get_thread_num();
+    int const dir = maxloc(dstregbbox.shape());
+    int const stride = dstregbbox.stride()[dir];
+    int const first = dstregbbox.lower()[dir];
+    int const last = dstregbbox.upper()[dir] + stride;
+    int const npoints = last - first;
+    int const mine = (npoints / stride + nthreads - 1) / nthreads * stride;
+    int const myfirst = std::min(last, first + me * mine);
+    int const mylast = std::min(last, myfirst + mine);
+    ibbox3 const myreg(dstregbbox.lower().replace(dir, myfirst),
+                       dstregbbox.upper().replace(dir, mylast - stride),
+                       dstregbbox.stride());
+    if (!myreg.empty()) {
+      try {
+        op(src, srcpadext, srcext, dst, dstpadext, dstext, srcbbox, dstbbox,
+           srcregbbox, myreg, nullptr);
+      } catch (std::exception const &e) {
+#pragma omp critical
+        err = e.what();
+      }
+    }
+  }
+  if (!err.empty())
+    throw std::runtime_error(err);
+}
+
+template <class F> int guarded(F f) {
+  try {
+    f();
+    return 0;
+  } catch (std::exception const &e) {
+    last_error = e.what();
+    return 1;
+  }
+}
+} // namespace
+
+#define OPARGS                                                                 \
+  const double *src, const int *srcpadext, const int *srcext, double *dst,     \
+      const int *dstpadext, const int *dstext, const int *srcbbox,             \
+      const int *dstbbox, const int *srcregbbox, const int *dstregbbox
+#define OPCALL                                                                 \
+  src, iv(srcpadext), iv(srcext), dst, iv(dstpadext), iv(dstext), ib(srcbbox), \
+      ib(dstbbox), ib(srcregbbox), ib(dstregbbox)
+
+extern "C" {
+
+const char *cgxref_last_error(void) { return last_error.c_str(); }
+void cgxref_set_openmp(int on) { cgx_shim_use_openmp = on; }
+
+// copy_3d (CarpetLib/src/copy_3d.cc:25-122); slab_offset may be NULL.
+int cgxref_copy_3d(OPARGS, const int *slab_offset) {
+  return guarded([&] {
+    islab slab;
+    if (slab_offset)
+      slab.offset = iv(slab_offset);
+    copy_3d<double>(OPCALL, slab_offset ? (void *)&slab : nullptr);
+  });
+}
+
+// prolongate_3d_rf2<double,ORDER> (CarpetLib/src/prolongate_3d_rf2.cc:356)
+int cgxref_prolongate_3d_rf2(int order, OPARGS) {
+  return guarded([&] {
+    op_t op = nullptr;
+    switch (order) {
+    case 1: op = &prolongate_3d_rf2<double, 1>; break;
+    case 3: op = &prolongate_3d_rf2<double, 3>; break;
+    case 5: op = &prolongate_3d_rf2<double, 5>; break;
+    case 7: op = &prolongate_3d_rf2<double, 7>; break;
+    case 9: op = &prolongate_3d_rf2<double, 9>; break;
+    case 11: op = &prolongate_3d_rf2<double, 11>; break;
+    default: throw std::runtime_error("no vertex-centred stencil of this order");
+    }
+    call_operator(op, OPCALL);
+  });
+}
+
+// prolongate_3d_cc_rf2<double,ORDER> (CarpetLib/src/prolongate_3d_cc_rf2.cc:238)
+int cgxref_prolongate_3d_cc_rf2(int order, OPARGS) {
+  return guarded([&] {
+    op_t op = nullptr;
+    switch (order) {
+    case 0: op = &prolongate_3d_cc_rf2<double, 0>; break;
+    case 1: op = &prolongate_3d_cc_rf2<double, 1>; break;
+    case 2: op = &prolongate_3d_cc_rf2<double, 2>; break;
+    case 3: op = &prolongate_3d_cc_rf2<double, 3>; break;
+    case 4: op = &prolongate_3d_cc_rf2<double, 4>; break;
+    case 5: op = &prolongate_3d_cc_rf2<double, 5>; break;
+    default: throw std::runtime_error("no cell-centred stencil of this order");
+    }
+    call_operator(op, OPCALL);
+  });
+}
+
+// restrict_3d_rf2 (CarpetLib/src/restrict_3d_rf2.cc:25); called directly,
+// as CarpetLib/src/data.cc:1041 does through call_operator.
+int cgxref_restrict_3d_rf2(OPARGS) {
+  return guarded([&] { call_operator(&restrict_3d_rf2<double>, OPCALL); });
+}
+
+// restrict_3d_cc_rf2 (CarpetLib/src/restrict_3d_cc_rf2.cc:23); CarpetLib
+// calls it without call_operator (data.cc:1100-1105).
+int cgxref_restrict_3d_cc_rf2(OPARGS) {
+  return guarded([&] { restrict_3d_cc_rf2<double>(OPCALL, nullptr); });
+}
+
+#define TIARGS                                                                 \
+  const int *srcpadext, const int *srcext, double *dst, double t,              \
+      const int *dstpadext, const int *dstext, const int *srcbbox,             \
+      const int *dstbbox, const int *srcregbbox, const int *dstregbbox
+#define TICALL                                                                 \
+  iv(srcpadext), iv(srcext), dst, t, iv(dstpadext), iv(dstext), ib(srcbbox),   \
+      ib(dstbbox), ib(srcregbbox), ib(dstregbbox), nullptr
+
+// The time interpolators open their own OpenMP region
+// (CarpetLib/src/interpolate_3d_2tl.cc:245, interpolate_3d_3tl.cc:385,
+// interpolate_eno_3d_3tl.cc:141).
+// interpolate_3d_2tl (CarpetLib/src/interpolate_3d_2tl.cc:24)
+int cgxref_interpolate_3d_2tl(const double *src1, double t1,
+                              const double *src2, double t2, TIARGS) {
+  return guarded(
+      [&] { interpolate_3d_2tl<double>(src1, t1, src2, t2, TICALL); });
+}
+
+// interpolate_3d_3tl (CarpetLib/src/interpolate_3d_3tl.cc:24)
+int cgxref_interpolate_3d_3tl(const double *src1, double t1,
+                              const double *src2, double t2,
+                              const double *src3, double t3, TIARGS) {
+  return guarded([&] {
+    interpolate_3d_3tl<double>(src1, t1, src2, t2, src3, t3, TICALL);
+  });
+}
+
+// interpolate_eno_3d_3tl (CarpetLib/src/interpolate_eno_3d_3tl.cc:32)
+int cgxref_interpolate_eno_3d_3tl(const double *src1, double t1,
+                                  const double *src2, double t2,
+                                  const double *src3, double t3, TIARGS) {
+  return guarded([&] {
+    interpolate_eno_3d_3tl<double>(src1, t1, src2, t2, src3, t3, TICALL);
+  });
+}
+
+} // extern "C"
