@@ -1,0 +1,461 @@
+#!/usr/bin/env python
+"""Benchmark: one coarse Berger-Oliger step of grid transfers.
+
+Workload (the 5-level order-5 hierarchy): 5 nested vertex-centred levels of
+129^3 points, each split into 2x2x2 components, 25 FP64 grid functions with
+3 timelevels, ghost width 3, buffer width 9; order-5 Lagrange boundary
+prolongation with quadratic time interpolation across 3 timelevels,
+injection restriction and ghost sync.  One step = every transfer of one
+coarse step (the finest level takes 16 substeps).  Inputs are seeded
+synthetic fields (4 Gaussians + 1e-6 noise).  Every step touches ~10 GB,
+far more than the 126 MB L2, so no flush is needed between steps.
+
+value        algorithmic GB/s of the batched form (one persistent kernel per
+             phase, the step replayed as CUDA graphs), inputs resident in HBM
+e2e          the same step through the public API with the grid data in
+             pinned host memory: H2D of every array the step reads and D2H of
+             every array it writes, inside the timed region
+plain        the plain per-box form (one launch per box-pair), same step
+roofline     the persistent kernel's algorithmic bytes / its CUDA-event time
+cpu_baseline CarpetLib's own operators (compiled from the reference) on the
+             host cores, a bounded sample of the same step
+
+--impl reference: only the CPU reference arm (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "prolong/restrict/sync GB/s & % HBM roof; batched+served vs plain; p50/p99 ms"
+WORKLOAD = "5 vc levels x 129^3 (2x2x2 comps), 25 GFs x 3 TLs, ghost 3, buffer 9, " \
+           "order-5 Lagrange + 3-TL time interpolation, rf2 injection, ghost sync; " \
+           "one coarse Berger-Oliger step"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=6)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="cgx", choices=["cgx", "reference"])
+    p.add_argument("--ngf", type=int, default=25)
+    p.add_argument("--npoints", type=int, default=129)
+    p.add_argument("--levels", type=int, default=5)
+    p.add_argument("--fp", default="fma", choices=["exact", "fma"])
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs"""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index, self.proc, self.lines = index, None, []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                smax = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------- field
+def gaussians(seed, L):
+    """4 Gaussians: centres ~U(domain), widths ~U(0.05,0.3) L, amplitudes ~U(-1,1)"""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return [(rng.uniform(0, L, 3), rng.uniform(0.05, 0.3) * L, rng.uniform(-1, 1))
+            for _ in range(4)]
+
+
+def fill_storage(st, h, seed=1):
+    import torch
+    L = h.levels[0].box[3]
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    for l, lev in enumerate(h.levels):
+        for tl in range(st.ntl):
+            for g in range(st.ngf):
+                gs = gaussians(seed * 1000 + g * 10 + tl, L)
+                for c, comp in enumerate(lev.comps):
+                    b = comp.exterior
+                    t = st.data[l][tl][g][c].tensor
+                    nz, ny, px = t.shape
+                    x = b[0] + torch.arange(px, device="cuda", dtype=torch.float64) * b[6]
+                    y = b[1] + torch.arange(ny, device="cuda", dtype=torch.float64) * b[7]
+                    z = b[2] + torch.arange(nz, device="cuda", dtype=torch.float64) * b[8]
+                    v = torch.zeros((nz, ny, px), dtype=torch.float64, device="cuda")
+                    for (cen, w, a) in gs:
+                        r2 = ((x - cen[0]) ** 2)[None, None, :] + ((y - cen[1]) ** 2)[None, :, None] \
+                            + ((z - cen[2]) ** 2)[:, None, None]
+                        v += a * torch.exp(-r2 / (w * w))
+                    v += 1e-6 * torch.randn((nz, ny, px), generator=gen, device="cuda",
+                                            dtype=torch.float64)
+                    t.copy_(v)
+
+
+# ----------------------------------------------------------------- CPU arm
+def coarse_points(reg, srcbbox, order=5):
+    """coarse points an order-5 vertex-centred prolongation of ``reg`` reads
+    (the algorithmic source bytes the library counts per timelevel)"""
+    lo1, hi1 = -(order // 2), order // 2 + 1
+    n = 1
+    for d in range(3):
+        soff = (reg[d] - srcbbox[d]) // reg[6 + d]
+        m = (reg[3 + d] - reg[d]) // reg[6 + d] + 1
+        cs = [(soff + i) for i in range(min(2, m))] + [(soff + i) for i in range(max(0, m - 2), m)]
+        lo = min((s >> 1) + (lo1 if s & 1 else 0) for s in cs)
+        hi = max((s >> 1) + (hi1 if s & 1 else 0) for s in cs)
+        n *= hi - lo + 1
+    return n
+
+
+def cpu_sample(h, ngf, seconds, prefer_ref=True):
+    """CarpetLib's operators on the host: the transfers of the finest level's
+    first two substeps (boundary prolongation with and without time
+    interpolation, sync) and one restriction, for as many grid functions as
+    fit the time budget.  Returns (GB/s, cores, kind, sample description)."""
+    import numpy as np
+    from oracle.binding import Port, Ref, alloc
+    from carpet_b200.hierarchy import npoints, size
+    if prefer_ref and Ref.available():
+        lib, kind = Ref(False), "reference"
+        lib.set_openmp(True)
+        cores = os.cpu_count()
+    else:
+        lib, kind = Port(), "port"
+        cores = 1
+    L = len(h.levels)
+    lf, lc = h.levels[L - 1], h.levels[L - 2]
+    rng = np.random.default_rng(7)
+
+    def arrays(lev):
+        return [alloc(c.exterior) for c in lev.comps]
+
+    def filled(lev):
+        out = arrays(lev)
+        for a in out:
+            a[...] = rng.standard_normal(a.shape)
+        return out
+
+    fine = filled(lf)
+    coarse = [filled(lc) for _ in range(3)]
+    dtc = 1.0 / 64
+    times = [0.0, -dtc, -2 * dtc]
+    tmp_cache = {}
+
+    def prolong(ntl):
+        by = 0
+        for p in h.prolong[L - 1]:
+            dst, db = fine[p.dst_comp], lf.comps[p.dst_comp].exterior
+            sb = lc.comps[p.src_comp].exterior
+            if ntl == 1:
+                lib.prolongate_3d_rf2(5, coarse[0][p.src_comp], sb, dst, db, p.dstbox)
+            else:
+                key = p.dstbox
+                if key not in tmp_cache:
+                    tmp_cache[key] = [alloc(p.dstbox, pad_x_even=False) for _ in range(3)]
+                tmps = tmp_cache[key]
+                for t in range(3):
+                    lib.prolongate_3d_rf2(5, coarse[t][p.src_comp], sb, tmps[t], p.dstbox, p.dstbox)
+                lib.interpolate_3d_3tl(tmps, times, p.dstbox, dst, db, p.dstbox, -dtc / 2)
+            by += 8 * npoints(p.dstbox) + ntl * 8 * coarse_points(p.dstbox, sb)
+        return by
+
+    def sync():
+        by = 0
+        for p in h.sync[L - 1]:
+            lib.copy_3d(fine[p.src_comp], lf.comps[p.src_comp].exterior, fine[p.dst_comp],
+                        lf.comps[p.dst_comp].exterior, p.srcbox, p.dstbox)
+            by += 16 * npoints(p.dstbox)
+        return by
+
+    def restrict():
+        by = 0
+        for p in h.restrict[L - 1]:
+            lib.restrict_3d_rf2(fine[p.src_comp], lf.comps[p.src_comp].exterior,
+                                coarse[0][p.dst_comp], lc.comps[p.dst_comp].exterior, p.dstbox)
+            by += 16 * npoints(p.dstbox)
+        return by
+
+    # one grid function's worth of the sample, repeated within the budget
+    t0 = time.perf_counter()
+    total, reps = 0, 0
+    while True:
+        total += prolong(3) + sync() + prolong(1) + sync() + restrict()
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or reps >= ngf:
+            break
+    el = time.perf_counter() - t0
+    sample = (f"finest level of the workload: 2 boundary prolongations (3-TL and 1-TL), "
+              f"2 syncs, 1 restriction; {reps} grid function(s); {total / 1e9:.2f} GB "
+              f"algorithmic in {el:.1f} s")
+    return total / el / 1e9, cores, kind, sample
+
+
+# ----------------------------------------------------------------- main
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from carpet_b200.hierarchy import nested
+        h = nested(args.levels, args.npoints, ghost=3, buffer=9, order=5)
+        vals = []
+        for s in range(args.warmup + args.steps):
+            gbs, cores, kind, sample = cpu_sample(h, args.ngf, args.cpu_seconds / 3)
+            if s >= args.warmup:
+                vals.append(gbs)
+        v = sorted(vals)[len(vals) // 2]
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "GB/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "parallelism": "host cores"},
+            "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import carpet_b200 as cb
+    from carpet_b200.amr import BergerOliger, Storage
+    from carpet_b200.hierarchy import nested
+
+    cb.set_fp_mode(args.fp == "fma")
+    h = nested(args.levels, args.npoints, ghost=3, buffer=9, order=5)
+    st = Storage(h, args.ngf, 3)
+    fill_storage(st, h, seed=1 + rank)
+    bo = BergerOliger(h, st, order_space=5, order_time=2)
+    steps3 = [bo.step_phases() for _ in range(3)]  # the rotation repeats every 3 steps
+    for keys in steps3:
+        for k in keys:
+            bo.batch(k)
+    stats = [bo.stats(k) for k in steps3]
+    bytes_step = sum(s["bytes"] for s in stats) / 3
+    points_step = sum(s["points"] for s in stats) / 3
+    launches_step = sum(s["launches"] for s in stats) / 3
+    stream = torch.cuda.Stream()
+    torch.cuda.synchronize()
+
+    # capture the three step variants as graphs
+    graphs = []
+    for keys in steps3:
+        g = cb.Graph()
+        with g.capture(stream):
+            bo.run(keys, stream)
+        graphs.append(g)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up, then K timed steps
+    for s in range(args.warmup):
+        graphs[s % 3].launch(stream)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        e0.record(stream)
+        for s in range(args.steps):
+            graphs[(args.warmup + s) % 3].launch(stream)
+        e1.record(stream)
+        stream.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    for b in bo.batches.values():
+        b.check(stream)
+    value = bytes_step * world / (ms * 1e-3) / 1e9
+    fine_pts = points_step * world / (ms * 1e-3)
+
+    # per-launch timing of the persistent kernel (same stream, no graph)
+    keys = steps3[(args.warmup + args.steps) % 3]
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in keys]
+    for (a, b_), k in zip(evs, keys):
+        a.record(stream)
+        bo.batch(k).launch(stream)
+        b_.record(stream)
+    stream.synchronize()
+    kt = sum(a.elapsed_time(b_) for a, b_ in evs) * 1e-3
+    kbytes = sum(bo.batch(k).stats()["bytes"] for k in keys)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = kbytes / kt / 1e9
+
+    # plain per-box form: one launch per box-pair, same step
+    plain = None
+    if not args.no_plain:
+        keys = steps3[0]
+        bo.run(keys, stream, per_box=True)  # warm
+        stream.synchronize()
+        a, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        bo.run(keys, stream, per_box=True)
+        b_.record(stream)
+        stream.synchronize()
+        pms = a.elapsed_time(b_)
+        plain = {"value": round(stats[0]["bytes"] / (pms * 1e-3) / 1e9, 3), "unit": "GB/s",
+                 "ms_per_step": round(pms, 3), "launches_per_step": stats[0]["pairs"]}
+
+    # end to end: grid data in pinned host memory; every step copies in all
+    # it reads and copies out all it writes (whole levels per timelevel)
+    e2e = None
+    if not args.no_e2e:
+        host = [[torch.empty_like(p, device="cpu").pin_memory() for p in lp] for lp in st.pools]
+        for lp, hp in zip(st.pools, host):
+            for p, q in zip(lp, hp):
+                q.copy_(p)
+        h2d = sum(p.numel() * 8 for lp in st.pools for p in lp)
+        d2h = sum(lp[0].numel() * 8 for lp in st.pools)
+        n_e2e = max(2, min(args.steps, 4))
+
+        def e2e_step(s):
+            keys = steps3[s % 3]
+            with torch.cuda.stream(stream):
+                for lp, hp in zip(st.pools, host):
+                    for p, q in zip(lp, hp):
+                        p.copy_(q, non_blocking=True)
+                graphs[s % 3].launch(stream)
+                for l, (lp, hp) in enumerate(zip(st.pools, host)):
+                    i = bo.pool_index(bo.rot[l], 0)
+                    hp[i].copy_(lp[i], non_blocking=True)
+            return keys
+
+        e2e_step(0)
+        stream.synchronize()
+        a, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for s in range(n_e2e):
+            e2e_step(s + 1)
+        b_.record(stream)
+        stream.synchronize()
+        ems = a.elapsed_time(b_) / n_e2e
+        if world > 1:
+            t = torch.tensor([ems], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": round(bytes_step * world / (ems * 1e-3) / 1e9, 3), "unit": "GB/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": round(ems, 3)}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        gbs, cores, kind, sample = cpu_sample(h, args.ngf, args.cpu_seconds)
+        cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": cores, "kind": kind,
+               "sample": sample}
+
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "k_batch_traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("bytes_per_launch_scaled")
+        except (OSError, ValueError):
+            traffic = None
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "fp_mode": args.fp, "ngf": args.ngf,
+                       "parallelism": "replicas" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (~10 GB per step)",
+                       "bytes_per_step": int(bytes_step), "fine_points_per_step": int(points_step),
+                       "resident_gb": round(st.nbytes() / 1e9, 2)},
+            "fine_points_per_s": round(fine_pts, 1),
+            "pct_hbm_roof": round(100 * value / world / peak, 2),
+            "pct_nominal_8tbs": round(100 * value / world / 8000.0, 2),
+            "plain": plain,
+            "batched_vs_plain": None if not plain else round(value / world / plain["value"], 2),
+            "gpu_launches": int(launches_step * args.steps),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "kernel": "k_batch (persistent, all phases)",
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"},
+            "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(),
+        }
+        print(json.dumps(out))
+    for g in graphs:
+        del g
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

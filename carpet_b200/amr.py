@@ -1,0 +1,204 @@
+"""Device-resident grid functions of a hierarchy and a Berger-Oliger driver.
+
+``Storage`` holds, for every level, ``ngf`` grid functions x ``ntl``
+timelevels x components, as ``Data`` arrays carved out of one device pool
+per (level, timelevel) -- the layout a CarpetLib ``ggf`` keeps as
+``storage[ml][rl][lc][tl]`` (CarpetLib/src/ggf.hh), packed so that a
+timelevel of a whole level is one contiguous block.  Cycling timelevels
+(ggf::cycle_all, CarpetLib/src/ggf.cc:248-267) is a rotation of which pool
+plays TL0/TL1/TL2, never a copy.
+
+``BergerOliger`` replays the transfer calls of one coarse Berger-Oliger
+step in Carpet's order (Carpet/src/Evolve.cc:44-121 with CallEvol
+369-454 and CallRestrict 456-583): every iteration of the finest level,
+each level whose step begins evolves -- cycle, boundary prolongation from
+the next coarser level at its new time (with time interpolation when the
+time falls between coarse timelevels), ghost sync -- and every level
+aligned at the end of the iteration receives the restriction from the next
+finer level followed by a sync.  The evolution itself (the right-hand
+side) is not part of the transfer path and is not run.
+
+Each such phase is one batch of box-pairs over all grid functions, run by
+the persistent kernel; a whole coarse step can be captured as a CUDA graph.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Dict, List, Tuple
+
+import numpy as np
+import torch
+
+from .hierarchy import Hierarchy, npoints, size
+from .transfer import OP_LAGRANGE, VERTEX, Batch, Data, Graph, _arrays, _stream
+from . import _lib
+import ctypes as C
+
+
+def _padded(ext_box):
+    nx, ny, nz = size(ext_box)
+    return nx + (nx & 1), ny, nz
+
+
+class Storage:
+    """[level][tl] -> one pool; data[level][tl][gf][comp] -> Data views"""
+
+    def __init__(self, h: Hierarchy, ngf: int, ntl: int, device="cuda"):
+        self.h, self.ngf, self.ntl = h, ngf, ntl
+        self.pools: List[List[torch.Tensor]] = []
+        self.data: List[List[List[List[Data]]]] = []
+        for lev in h.levels:
+            shapes = [_padded(c.exterior) for c in lev.comps]
+            # 256-byte aligned offsets for every component array
+            offs, n = [], 0
+            for _ in range(ngf):
+                row = []
+                for (px, py, pz) in shapes:
+                    row.append(n)
+                    n += ((px * py * pz + 31) // 32) * 32
+                offs.append(row)
+            lp, ld = [], []
+            for tl in range(ntl):
+                pool = torch.empty(n, dtype=torch.float64, device=device)
+                lp.append(pool)
+                gfs = []
+                for g in range(ngf):
+                    comps = []
+                    for c, (px, py, pz) in enumerate(shapes):
+                        o = offs[g][c]
+                        t = pool[o:o + px * py * pz].view(pz, py, px)
+                        comps.append(Data(lev.comps[c].exterior, t))
+                    gfs.append(comps)
+                ld.append(gfs)
+            self.pools.append(lp)
+            self.data.append(ld)
+
+    def nbytes(self) -> int:
+        return sum(p.numel() * 8 for lp in self.pools for p in lp)
+
+    def fill(self, fn, seed=0):
+        """fn(x, y, z, gf, tl, rng) -> values, evaluated on every array"""
+        rng = np.random.default_rng(seed)
+        for l, lev in enumerate(self.h.levels):
+            for tl in range(self.ntl):
+                for g in range(self.ngf):
+                    for c, comp in enumerate(lev.comps):
+                        b = comp.exterior
+                        nx, ny, nz = size(b)
+                        x = b[0] + np.arange(nx) * b[6]
+                        y = b[1] + np.arange(ny) * b[7]
+                        z = b[2] + np.arange(nz) * b[8]
+                        Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+                        v = fn(X, Y, Z, g, tl, rng)
+                        t = self.data[l][tl][g][c].tensor
+                        full = np.zeros(tuple(t.shape))
+                        full[:, :, :nx] = v
+                        t.copy_(torch.from_numpy(full))
+
+
+@dataclass
+class Phase:
+    kind: str          # "prolong", "sync", "restrict"
+    level: int         # destination level
+    rot: Tuple[int, ...]  # rotation of the levels involved
+    ntl: int           # timelevels read (prolongation: 1 or 3)
+
+
+class BergerOliger:
+    """Transfer phases of one coarse step of a nested hierarchy."""
+
+    def __init__(self, h: Hierarchy, st: Storage, order_space=5, order_time=2,
+                 op=OP_LAGRANGE, cent=VERTEX):
+        self.h, self.st = h, st
+        self.order_space, self.order_time = order_space, order_time
+        self.op, self.cent = op, cent
+        self.L = len(h.levels)
+        self.batches: Dict[tuple, Batch] = {}
+        self.rot = [0] * self.L  # cycles of each level modulo ntl
+
+    # which pool holds timelevel tl of level l under rotation r
+    def pool_index(self, r: int, tl: int) -> int:
+        return (tl - r) % self.st.ntl
+
+    def _tl(self, l, r, tl):
+        return self.st.data[l][self.pool_index(r, tl)]
+
+    def _build(self, key) -> Batch:
+        kind, l, rots, ntl = key
+        b = Batch()
+        h, st = self.h, self.st
+        if kind == "sync":
+            r, = rots
+            arrs = self._tl(l, r, 0)
+            for g in range(st.ngf):
+                for p in h.sync[l]:
+                    b.add(arrs[g][p.dst_comp], [arrs[g][p.src_comp]], [0.0], p.dstbox, p.srcbox,
+                          0.0, 1, 0, op=self.op, cent=self.cent)
+        elif kind == "prolong":
+            rf, rc = rots
+            dst = self._tl(l, rf, 0)
+            srcs = [self._tl(l - 1, rc, t) for t in range(st.ntl)]
+            # coarse timelevels at 0, -dt, -2dt; the fine level sits half a
+            # coarse step back (between timelevels) or on TL0
+            dtc = 1.0 / 64
+            times = [0.0, -dtc, -2 * dtc]
+            time = -dtc / 2 if ntl > 1 else 0.0
+            for g in range(st.ngf):
+                for p in h.prolong[l]:
+                    b.add(dst[g][p.dst_comp], [s[g][p.src_comp] for s in srcs], times,
+                          p.dstbox, p.srcbox, time, self.order_space, self.order_time,
+                          op=self.op, cent=self.cent)
+        elif kind == "restrict":
+            rc, rf = rots
+            dst = self._tl(l, rc, 0)
+            src = self._tl(l + 1, rf, 0)
+            for g in range(st.ngf):
+                for p in h.restrict[l + 1]:
+                    b.add(dst[g][p.dst_comp], [src[g][p.src_comp]], [0.0], p.dstbox, p.srcbox,
+                          0.0, self.order_space, 0, op=self.op, cent=self.cent)
+        b.upload()
+        return b
+
+    def batch(self, key) -> Batch:
+        if key not in self.batches:
+            self.batches[key] = self._build(key)
+        return self.batches[key]
+
+    def step_phases(self) -> List[tuple]:
+        """the phases of one coarse step, advancing the rotation state"""
+        L = self.L
+        nit = 2 ** (L - 1)
+        keys = []
+        for it in range(1, nit + 1):
+            for l in range(L):
+                every = 2 ** (L - 1 - l)
+                if (it - 1) % every == 0:
+                    self.rot[l] = (self.rot[l] + 1) % self.st.ntl  # cycle_all
+                    if l > 0:
+                        # odd substeps of level l fall between coarse times
+                        sub = ((it - 1) // every) % 2
+                        ntl = 3 if sub == 0 else 1
+                        keys.append(("prolong", l, (self.rot[l], self.rot[l - 1]), ntl))
+                    keys.append(("sync", l, (self.rot[l],), 1))
+            for l in range(L - 2, -1, -1):
+                if it % (2 ** (L - 1 - l)) == 0:
+                    keys.append(("restrict", l, (self.rot[l], self.rot[l + 1]), 1))
+                    keys.append(("sync", l, (self.rot[l],), 1))
+        return keys
+
+    def run(self, keys, stream=None, per_box=False):
+        for k in keys:
+            b = self.batch(k)
+            if per_box:
+                b.launch_per_box(stream)
+            else:
+                b.launch(stream)
+
+    def stats(self, keys):
+        tot = dict(pairs=0, tiles=0, points=0, bytes=0, launches=0)
+        for k in keys:
+            s = self.batch(k).stats()
+            for n in ("pairs", "tiles", "points", "bytes"):
+                tot[n] += s[n]
+            tot["launches"] += 1
+        return tot

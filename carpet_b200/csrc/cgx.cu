@@ -1,0 +1,873 @@
+// cgx.cu -- kernels and host side of the C-ABI in include/cgx.h.
+//
+// Host side: restates the argument handling of CarpetLib's transfer path --
+// gdata::transfer_data / find_source_timelevel (CarpetLib/src/gdata.cc:124-349)
+// and data<T>::transfer_time / transfer_p_r / transfer_prolongate /
+// transfer_restrict / time_interpolate (CarpetLib/src/data.cc:485-1299) --
+// and turns one box-pair into one device descriptor (cgx::Desc).  The
+// reference aborts on bad arguments; here every check returns a status.
+//
+// Device side: cgx_device.cuh.  Two kernels run the same tile routines:
+//   k_pair   grid = the tiles of one descriptor (the plain per-box form);
+//   k_batch  persistent, one CTA per SM slot, tiles of many descriptors
+//            taken from a device work counter.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cgx.h"
+#include "cgx_device.cuh"
+
+using namespace cgx;
+
+// ============================================================== device side
+namespace {
+
+__device__ __forceinline__ void report(int *status, int code) {
+  if (status) atomicCAS(status, 0, code);
+}
+
+// dynamic shared memory of the largest variant a kernel dispatches
+template <int MAXORDER> constexpr int smem_doubles() {
+  return PSmem<VC<MAXORDER>, 3>::total > PSmem<CC<5>, 3>::total
+             ? PSmem<VC<MAXORDER>, 3>::total
+             : PSmem<CC<5>, 3>::total;
+}
+
+template <class F, int FMA>
+__device__ __forceinline__ void prolong_ntl(const Desc &d, int tile, double *sm) {
+  switch (d.ntl) {
+  case 1: prolong_tile<F, FMA, 1, T_NONE>(d, tile, sm); break;
+  case 2: prolong_tile<F, FMA, 2, T_LIN>(d, tile, sm); break;
+  default:
+    if (d.tkind == T_ENO) prolong_tile<F, FMA, 3, T_ENO>(d, tile, sm);
+    else prolong_tile<F, FMA, 3, T_QUAD>(d, tile, sm);
+  }
+}
+
+// HIGH selects the vertex-centred orders 7/9/11, which live in their own
+// kernel so that their larger register windows do not lower the occupancy
+// of the common orders.
+template <int FMA, bool HIGH>
+__device__ __forceinline__ void run_tile(const Desc &d, int tile, double *sm, int *status) {
+  switch (d.kind) {
+  case K_COPY:
+    if (d.ntl == 1) copy_tile<FMA, 1, T_NONE>(d, tile);
+    else if (d.ntl == 2) copy_tile<FMA, 2, T_LIN>(d, tile);
+    else if (d.tkind == T_ENO) copy_tile<FMA, 3, T_ENO>(d, tile);
+    else copy_tile<FMA, 3, T_QUAD>(d, tile);
+    return;
+  case K_RESTRICT_VC: restrict_vc_tile(d, tile); return;
+  case K_RESTRICT_CC: restrict_cc_tile<FMA>(d, tile); return;
+  case K_PROLONG_VC:
+    if (HIGH) {
+      switch (d.order) {
+      case 7: prolong_ntl<VC<7>, FMA>(d, tile, sm); return;
+      case 9: prolong_ntl<VC<9>, FMA>(d, tile, sm); return;
+      case 11: prolong_ntl<VC<11>, FMA>(d, tile, sm); return;
+      }
+    } else {
+      switch (d.order) {
+      case 1: prolong_ntl<VC<1>, FMA>(d, tile, sm); return;
+      case 3: prolong_ntl<VC<3>, FMA>(d, tile, sm); return;
+      case 5: prolong_ntl<VC<5>, FMA>(d, tile, sm); return;
+      }
+    }
+    break;
+  case K_PROLONG_CC:
+    if (!HIGH) {
+      switch (d.order) {
+      case 0: prolong_ntl<CC<0>, FMA>(d, tile, sm); return;
+      case 1: prolong_ntl<CC<1>, FMA>(d, tile, sm); return;
+      case 2: prolong_ntl<CC<2>, FMA>(d, tile, sm); return;
+      case 3: prolong_ntl<CC<3>, FMA>(d, tile, sm); return;
+      case 4: prolong_ntl<CC<4>, FMA>(d, tile, sm); return;
+      case 5: prolong_ntl<CC<5>, FMA>(d, tile, sm); return;
+      }
+    }
+    break;
+  case K_PROLONG_ENO:
+    if (!HIGH) { prolong_ntl<ENO, FMA>(d, tile, sm); return; }
+    break;
+  }
+  if (threadIdx.x == 0) report(status, CGX_EDEVICE);
+}
+
+template <int FMA, bool HIGH>
+__global__ void __launch_bounds__(NTHREADS, 2)
+    k_pair(const __grid_constant__ Desc d, int *status) {
+  extern __shared__ double sm[];
+  run_tile<FMA, HIGH>(d, blockIdx.x, sm, status);
+}
+
+// Persistent form: each CTA repeatedly claims the next tile index from
+// *counter; prefix[i] is the first global tile of descriptor i.
+template <int FMA>
+__global__ void __launch_bounds__(NTHREADS, 2)
+    k_batch(const Desc *__restrict__ descs, const long long *__restrict__ prefix, int ndesc,
+            long long ntiles, unsigned long long *counter, int *status) {
+  extern __shared__ double sm[];
+  __shared__ long long s_tile;
+  __shared__ int s_desc;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      long long t = (long long)atomicAdd(counter, 1ULL);
+      int lo = 0, hi = ndesc - 1;
+      if (t < ntiles) {
+        while (lo < hi) { // last descriptor with prefix <= t
+          int mid = (lo + hi + 1) >> 1;
+          if (prefix[mid] <= t) lo = mid;
+          else hi = mid - 1;
+        }
+      }
+      s_tile = t;
+      s_desc = lo;
+    }
+    __syncthreads();
+    const long long t = s_tile;
+    const int di = s_desc;
+    __syncthreads(); // everyone has read s_tile before thread 0 rewrites it
+    if (t >= ntiles) break;
+    run_tile<FMA, false>(descs[di], (int)(t - prefix[di]), sm, status);
+  }
+}
+
+} // namespace
+
+// ============================================================== host side
+namespace {
+
+thread_local std::string g_err;
+int g_fp_mode = CGX_FP_EXACT;
+bool g_attr_done[2][2] = {{false, false}, {false, false}};
+bool g_batch_attr_done[2] = {false, false};
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char *what) {
+  return fail(CGX_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+struct Box {
+  int lo[3], up[3], str[3];
+  explicit Box(const int *b) {
+    for (int d = 0; d < 3; ++d) { lo[d] = b[d]; up[d] = b[3 + d]; str[d] = b[6 + d]; }
+  }
+  Box() = default;
+  bool empty() const {
+    for (int d = 0; d < 3; ++d) if (lo[d] > up[d]) return true;
+    return false;
+  }
+  int size(int d) const { return empty() ? 0 : (up[d] - lo[d] + str[d]) / str[d]; }
+  long long npoints() const { return (long long)size(0) * size(1) * size(2); }
+  // bbox::is_contained_in (bbox.cc:103-109): no alignment check
+  bool in(const Box &b) const {
+    if (empty()) return true;
+    for (int d = 0; d < 3; ++d) if (lo[d] < b.lo[d] || up[d] > b.up[d]) return false;
+    return true;
+  }
+  bool stride_eq(const Box &b) const {
+    for (int d = 0; d < 3; ++d) if (str[d] != b.str[d]) return false;
+    return true;
+  }
+};
+
+int kind_tiles(int kind, const int *n, int *tiles) {
+  bool prol = kind == K_PROLONG_VC || kind == K_PROLONG_CC || kind == K_PROLONG_ENO;
+  const int t[3] = {prol ? PTX : CTX, prol ? PTY : CTY, prol ? PTZ : CTZ};
+  long long tot = 1;
+  for (int d = 0; d < 3; ++d) { tiles[d] = (n[d] + t[d] - 1) / t[d]; tot *= tiles[d]; }
+  return tot > 0x7fffffff ? -1 : (int)tot;
+}
+
+// gdata::find_source_timelevel, CarpetLib/src/gdata.cc:288-349
+int find_tl(const double *times, int ntimes, double time, int order_time, int op, int *tl0,
+            int *ntl) {
+  if (ntimes <= 0 || order_time < 0 || !times)
+    return fail(CGX_EINVAL, "find_source_timelevel: no timelevels");
+  const double eps = 1.0e-12;
+  double mn = times[0], mx = times[0];
+  for (int i = 1; i < ntimes; ++i) { mn = std::min(mn, times[i]); mx = std::max(mx, times[i]); }
+  const double some_time = std::fabs(mn) + std::fabs(mx) + 1.0;
+  if (op != CGX_OP_COPY && (time < mn - eps * some_time || time > mx + eps * some_time))
+    return fail(CGX_EINVAL, "find_source_timelevel: extrapolation in time (time=%.17g)", time);
+  int tl = -1;
+  if (ntimes == 1) tl = 0;
+  if (tl == -1 && op == CGX_OP_COPY) tl = 0;
+  if (tl == -1)
+    for (int i = 0; i < ntimes; ++i)
+      if (std::fabs(times[i] - time) < eps * some_time) { tl = i; break; }
+  if (tl >= 0) { *tl0 = tl; *ntl = 1; }
+  else { *tl0 = 0; *ntl = order_time + 1; }
+  if (*tl0 + *ntl > ntimes)
+    return fail(CGX_EINVAL, "find_source_timelevel: %d timelevels needed, %d given", *tl0 + *ntl,
+                ntimes);
+  return CGX_OK;
+}
+
+// Time weights exactly as the reference computes them (once per call):
+// interpolate_3d_2tl.cc:232-242, interpolate_3d_3tl.cc:365-382,
+// interpolate_eno_3d_3tl.cc:105-135.
+int time_weights(int tk, const double *ts, double t, double *w) {
+  if (tk == T_LIN) {
+    const double t1 = ts[0], t2 = ts[1], eps = 1.0e-12;
+    if (std::fabs(t1 - t2) < eps) return fail(CGX_EINVAL, "interpolate_3d_2tl: arrays have same time");
+    if (t < std::min(t1, t2) - eps || t > std::max(t1, t2) + eps)
+      return fail(CGX_EINVAL, "interpolate_3d_2tl: extrapolation in time");
+    w[0] = (t - t2) / (t1 - t2);
+    w[1] = (t - t1) / (t2 - t1);
+    return CGX_OK;
+  }
+  const double t1 = ts[0], t2 = ts[1], t3 = ts[2];
+  if (tk == T_QUAD) {
+    const double eps = 1.0e-12;
+    if (std::fabs(t1 - t2) < eps || std::fabs(t1 - t3) < eps || std::fabs(t2 - t3) < eps)
+      return fail(CGX_EINVAL, "interpolate_3d_3tl: arrays have same time");
+    if (t < std::fmin(std::fmin(t1, t2), t3) - eps || t > std::fmax(std::fmax(t1, t2), t3) + eps)
+      return fail(CGX_EINVAL, "interpolate_3d_3tl: extrapolation in time");
+  } else {
+    const double tmin = std::min(t1, std::min(t2, t3)), tmax = std::max(t1, std::max(t2, t3));
+    const double eps = 1.0e-12 * (tmax - tmin);
+    if (std::fabs(t1 - t2) < eps || std::fabs(t1 - t3) < eps || std::fabs(t2 - t3) < eps)
+      return fail(CGX_EINVAL, "interpolate_eno_3d_3tl: arrays have same time");
+    if (t < tmin - eps || t > tmax + eps)
+      return fail(CGX_EINVAL, "interpolate_eno_3d_3tl: extrapolation in time");
+    w[3] = (t - t2) / (t1 - t2);
+    w[4] = (t - t1) / (t2 - t1);
+    w[5] = (t - t3) / (t2 - t3);
+    w[6] = (t - t2) / (t3 - t2);
+    const bool use12 = t >= std::min(t1, t2) - eps && t <= std::max(t1, t2) + eps;
+    const bool use23 = t >= std::min(t2, t3) - eps && t <= std::max(t2, t3) + eps;
+    if (!use12 && !use23) return fail(CGX_EINVAL, "interpolate_eno_3d_3tl: no bracketing pair");
+    w[7] = use12 ? 1.0 : 0.0;
+  }
+  w[0] = (t - t2) * (t - t3) / ((t1 - t2) * (t1 - t3));
+  w[1] = (t - t1) * (t - t3) / ((t2 - t1) * (t2 - t3));
+  w[2] = (t - t1) * (t - t2) / ((t3 - t1) * (t3 - t2));
+  return CGX_OK;
+}
+
+// Coarse window [lo, hi] of one parity relative to the coarse base c.
+struct Win { int lo0, hi0, lo1, hi1; };
+Win family_window(int kind, int order) {
+  if (kind == K_PROLONG_VC) { int lo = -((order + 1) / 2) + 1; return {0, 0, lo, lo + order}; }
+  if (kind == K_PROLONG_CC) {
+    int n = order + 1, lo0 = -n / 2, lo1 = -n / 2 + (order % 2 ? 1 : 0);
+    return {lo0, lo0 + n - 1, lo1, lo1 + n - 1};
+  }
+  return {0, 0, -1, 2}; // ENO
+}
+
+// Every coarse point any fine point of the region reads: the first two and
+// last two fine points of each axis bound it.  Used for the exact in-bounds
+// check (stricter than the reference's expand() test, which works in fine
+// strides) and for the algorithmic byte count.
+void stencil_range(const Win &w, int soff, int n, int *cmin, int *cmax) {
+  int mn = 1 << 30, mx = -(1 << 30);
+  for (int i = 0; i < n; i = (i == 1 && n > 3) ? n - 2 : i + 1) {
+    int s = soff + i, c = s >> 1, p = s & 1;
+    mn = std::min(mn, c + (p ? w.lo1 : w.lo0));
+    mx = std::max(mx, c + (p ? w.hi1 : w.hi0));
+  }
+  *cmin = mn;
+  *cmax = mx;
+}
+
+struct Built {
+  Desc d;
+  long long bytes;  // algorithmic bytes (reads + writes)
+  long long points; // destination points written
+  int ntiles;
+};
+
+bool pad_ok(const cgx_array *a) {
+  Box b(a->bbox);
+  for (int d = 0; d < 3; ++d) {
+    if (b.str[d] <= 0) return false;
+    if (a->padext[d] < b.size(d)) return false;
+  }
+  return a->data != nullptr;
+}
+
+// The spatial operator of one timelevel: transfer_p_r (data.cc:537-556).
+// regdst: the destination bbox the operator sees (dst extent, or dstbox
+// itself for the temporaries of data.cc:506-509).
+int build_spatial(int op, int cent, const cgx_array *dst, const cgx_array *src,
+                  const Box &regdst, const Box &dstbox, const Box &srcbox, const int *slab,
+                  int order_space, Built *out) {
+  Desc &d = out->d;
+  Box sb(src->bbox), db(dst->bbox);
+  bool eq = true, gt = true, lt = true;
+  for (int k = 0; k < 3; ++k) {
+    eq &= sb.str[k] == regdst.str[k];
+    gt &= sb.str[k] > regdst.str[k];
+    lt &= sb.str[k] < regdst.str[k];
+  }
+  for (int k = 0; k < 3; ++k) d.sext[k] = sb.size(k);
+  d.ssy = src->padext[0];
+  d.ssz = (long long)src->padext[0] * src->padext[1];
+  if (eq) {
+    // copy_from_innerloop -> copy_3d (copy_3d.cc:36-82)
+    const Box &reg = dstbox;
+    if (!sb.stride_eq(reg) || !regdst.stride_eq(reg) || !srcbox.stride_eq(reg))
+      return fail(CGX_EINVAL, "copy_3d: strides disagree");
+    if (reg.empty()) return fail(CGX_EINVAL, "copy_3d: region extent is empty");
+    Box sreg = reg;
+    if (slab)
+      for (int k = 0; k < 3; ++k) { sreg.lo[k] += slab[k] * reg.str[k]; sreg.up[k] += slab[k] * reg.str[k]; }
+    if (!sreg.in(srcbox)) return fail(CGX_EINVAL, "copy_3d: shifted source region outside srcbox");
+    if (!sreg.in(sb) || !reg.in(regdst))
+      return fail(CGX_EINVAL, "copy_3d: region extent is not contained in array extent");
+    for (int k = 0; k < 3; ++k) {
+      if ((sreg.lo[k] - sb.lo[k]) % sb.str[k] || (reg.lo[k] - regdst.lo[k]) % regdst.str[k])
+        return fail(CGX_EINVAL, "copy_3d: region not aligned with the arrays");
+      d.n[k] = reg.size(k);
+      d.soff[k] = (sreg.lo[k] - sb.lo[k]) / sb.str[k];
+    }
+    d.kind = K_COPY;
+    d.order = 0;
+    out->points = reg.npoints();
+    out->bytes = 16 * out->points;
+    return CGX_OK;
+  }
+  if (gt) {
+    if (op == CGX_OP_SYNC || op == CGX_OP_RESTRICT)
+      return fail(CGX_EINVAL, "transfer_p_r: prolongation with a sync/restrict operator");
+    if (slab) return fail(CGX_EINVAL, "transfer_p_r: slab with prolongation");
+    const Box &reg = dstbox;
+    int kind;
+    if (op == CGX_OP_COPY || op == CGX_OP_LAGRANGE) {
+      if (cent == CGX_VERTEX) {
+        if (order_space != 1 && order_space != 3 && order_space != 5 && order_space != 7 &&
+            order_space != 9 && order_space != 11)
+          return fail(CGX_EINVAL, "transfer_prolongate: no vertex-centred stencil of order %d",
+                      order_space);
+        kind = K_PROLONG_VC;
+      } else if (cent == CGX_CELL) {
+        if (order_space < 0 || order_space > 5)
+          return fail(CGX_EINVAL, "transfer_prolongate: no cell-centred stencil of order %d",
+                      order_space);
+        kind = K_PROLONG_CC;
+      } else return fail(CGX_EINVAL, "transfer_prolongate: bad centering");
+    } else if (op == CGX_OP_ENO) {
+      if (cent != CGX_VERTEX)
+        return fail(CGX_EUNSUPPORTED, "transfer_prolongate: cell-centred ENO is not provided");
+      if (order_space != 3 && order_space != 5) // data.cc:660-686
+        return fail(CGX_EINVAL, "transfer_prolongate: no ENO stencil of order %d", order_space);
+      kind = K_PROLONG_ENO;
+    } else return fail(CGX_EUNSUPPORTED, "transfer_prolongate: operator %d is not provided", op);
+
+    // argument checks of prolongate_3d_rf2.cc:373-417,
+    // prolongate_3d_cc_rf2.cc:253-321, prolongate_3d_real8_eno.F90:122-175
+    for (int k = 0; k < 3; ++k) {
+      if (sb.str[k] <= reg.str[k] || regdst.str[k] != reg.str[k])
+        return fail(CGX_EINVAL, "prolongate: strides disagree");
+      if (sb.str[k] != 2 * regdst.str[k])
+        return fail(CGX_EINVAL, "prolongate: source strides are not twice the destination strides");
+      if (kind != K_PROLONG_CC &&
+          (sb.lo[k] % sb.str[k] || regdst.lo[k] % regdst.str[k] || reg.lo[k] % reg.str[k]))
+        return fail(CGX_EINVAL, "prolongate: bbox is not aligned with vertices");
+      if (kind == K_PROLONG_CC && regdst.str[k] % 2)
+        return fail(CGX_EINVAL, "prolongate_3d_cc_rf2: destination strides are not even");
+    }
+    if (reg.empty()) return fail(CGX_EINVAL, "prolongate: region extent is empty");
+    if (!reg.in(regdst)) return fail(CGX_EINVAL, "prolongate: region extent is not contained in array extent");
+    const Win w = family_window(kind, order_space);
+    long long ncoarse = 1;
+    for (int k = 0; k < 3; ++k) {
+      const int h = kind == K_PROLONG_CC ? reg.str[k] / 2 : 0;
+      if ((reg.lo[k] - sb.lo[k] + h) % reg.str[k] || (reg.lo[k] - regdst.lo[k]) % reg.str[k])
+        return fail(CGX_EINVAL, "prolongate: region not aligned with the arrays");
+      d.n[k] = reg.size(k);
+      d.soff[k] = (reg.lo[k] - sb.lo[k] + h) / reg.str[k];
+      if (d.soff[k] < 0) return fail(CGX_EINVAL, "prolongate: region extent is not contained in array extent");
+      int cmin, cmax;
+      stencil_range(w, d.soff[k], d.n[k], &cmin, &cmax);
+      if (cmin < 0 || cmax >= sb.size(k))
+        return fail(CGX_EINVAL, "prolongate: stencil reaches outside the source array "
+                                "(axis %d, coarse %d..%d of %d)", k, cmin, cmax, sb.size(k));
+      ncoarse *= cmax - cmin + 1;
+    }
+    // the reference's own containment test (expand in fine strides)
+    if (kind == K_PROLONG_VC) {
+      Box ex = reg;
+      for (int k = 0; k < 3; ++k) {
+        int n = reg.size(k);
+        bool nlo = d.soff[k] % 2 != 0, nhi = (d.soff[k] + n - 1) % 2 != 0;
+        int olo = nlo ? order_space / 2 + 1 : (n > 1 ? order_space / 2 : 0);
+        int ohi = nhi ? order_space / 2 + 1 : (n > 1 ? order_space / 2 : 0);
+        ex.lo[k] -= olo * reg.str[k];
+        ex.up[k] += ohi * reg.str[k];
+      }
+      if (!ex.in(sb)) return fail(CGX_EINVAL, "prolongate_3d_rf2: region extent is not contained in array extent");
+    }
+    d.kind = kind;
+    d.order = order_space;
+    out->points = reg.npoints();
+    out->bytes = 8 * out->points + 8 * ncoarse; // per timelevel source added by caller
+    return CGX_OK;
+  }
+  if (lt) {
+    if (op == CGX_OP_SYNC) return fail(CGX_EINVAL, "transfer_p_r: restriction with a sync operator");
+    if (!(op == CGX_OP_COPY || op == CGX_OP_LAGRANGE || op == CGX_OP_ENO || op == CGX_OP_WENO ||
+          op == CGX_OP_TVD || op == CGX_OP_LAGRANGE_MONOTONE || op == CGX_OP_RESTRICT))
+      return fail(CGX_EUNSUPPORTED, "transfer_restrict: operator %d is not provided", op);
+    const Box &reg = dstbox;
+    // restrict_3d_rf2.cc:38-68, restrict_3d_cc_rf2.cc:172-207
+    for (int k = 0; k < 3; ++k) {
+      if (sb.str[k] >= reg.str[k] || regdst.str[k] != reg.str[k])
+        return fail(CGX_EINVAL, "restrict: strides disagree");
+      if (2 * sb.str[k] != regdst.str[k])
+        return fail(CGX_EINVAL, "restrict: destination strides are not twice the source strides");
+    }
+    if (reg.empty()) return fail(CGX_EINVAL, "restrict: region extent is empty");
+    if (cent == CGX_VERTEX) {
+      if (slab) return fail(CGX_EINVAL, "transfer_restrict: slab with restriction");
+      if (!reg.in(sb) || !reg.in(regdst))
+        return fail(CGX_EINVAL, "restrict_3d_rf2: region extent is not contained in array extent");
+      for (int k = 0; k < 3; ++k) {
+        if ((reg.lo[k] - sb.lo[k]) % sb.str[k] || (reg.lo[k] - regdst.lo[k]) % regdst.str[k])
+          return fail(CGX_EINVAL, "restrict_3d_rf2: region not aligned");
+        d.n[k] = reg.size(k);
+        d.soff[k] = (reg.lo[k] - sb.lo[k]) / sb.str[k];
+        if (d.soff[k] + 2 * (d.n[k] - 1) >= sb.size(k))
+          return fail(CGX_EINVAL, "restrict_3d_rf2: region extent is not contained in array extent");
+      }
+      d.kind = K_RESTRICT_VC;
+      out->points = reg.npoints();
+      out->bytes = 16 * out->points;
+    } else if (cent == CGX_CELL) {
+      // bbox::expanded_for (bbox.cc:208-219) of the region onto the source
+      Box ef = reg;
+      for (int k = 0; k < 3; ++k) {
+        int s = sb.str[k];
+        auto imod = [](int x, int y) { int r = x % y; return r < 0 ? r + y : r; };
+        int loff = imod(reg.lo[k] - sb.lo[k], s), uoff = imod(reg.up[k] - sb.lo[k], s);
+        ef.lo[k] = reg.lo[k] - loff;
+        ef.up[k] = reg.up[k] + (s - uoff) % s;
+        ef.str[k] = s;
+      }
+      if (!ef.in(sb) || !reg.in(regdst))
+        return fail(CGX_EINVAL, "restrict_3d_cc_rf2: region extent is not contained in array extent");
+      for (int k = 0; k < 3; ++k) {
+        int h = sb.str[k] / 2;
+        if (sb.str[k] % 2 || (reg.lo[k] - sb.lo[k] - h) % sb.str[k] ||
+            (reg.lo[k] - regdst.lo[k]) % regdst.str[k])
+          return fail(CGX_EINVAL, "restrict_3d_cc_rf2: region not aligned");
+        d.n[k] = reg.size(k);
+        d.soff[k] = (reg.lo[k] - sb.lo[k] - h) / sb.str[k];
+        if (d.soff[k] < 0 || d.soff[k] + 2 * d.n[k] - 1 >= sb.size(k))
+          return fail(CGX_EINVAL, "restrict_3d_cc_rf2: region extent is not contained in array extent");
+      }
+      d.kind = K_RESTRICT_CC;
+      out->points = reg.npoints();
+      out->bytes = 72 * out->points;
+    } else return fail(CGX_EINVAL, "transfer_restrict: bad centering");
+    d.order = 0;
+    return CGX_OK;
+  }
+  return fail(CGX_EINVAL, "transfer_p_r: mixed strides");
+}
+
+// One box-pair: gdata::transfer_data on one process + transfer_time.
+int build(int op, int cent, const cgx_array *dst, const cgx_array *srcs, const double *times,
+          int nsrc, const int *dstbox_, const int *srcbox_, const int *slab, double time,
+          int order_space, int order_time, Built *out) {
+  if (!dst || !srcs || !dstbox_ || !srcbox_) return fail(CGX_EINVAL, "transfer: null argument");
+  if (op == CGX_OP_ERROR || op == CGX_OP_NONE)
+    return fail(CGX_EINVAL, "transfer_data: operator is none/error");
+  if (nsrc < 1 || nsrc > 16) return fail(CGX_EINVAL, "transfer_data: bad number of sources");
+  if (!pad_ok(dst)) return fail(CGX_EINVAL, "transfer: bad destination array");
+  for (int t = 0; t < nsrc; ++t) {
+    if (!pad_ok(&srcs[t])) return fail(CGX_EINVAL, "transfer: bad source array %d", t);
+    for (int k = 0; k < 3; ++k)
+      if (srcs[t].padext[k] != srcs[0].padext[k])
+        return fail(CGX_EINVAL, "transfer: source timelevels differ in shape");
+    for (int k = 0; k < 9; ++k)
+      if (srcs[t].bbox[k] != srcs[0].bbox[k])
+        return fail(CGX_EINVAL, "transfer: source timelevels differ in extent");
+  }
+  const Box dstbox(dstbox_), srcbox(srcbox_), db(dst->bbox);
+  // gdata.cc:139-147
+  if (dstbox.empty()) return fail(CGX_EINVAL, "transfer_data: empty dstbox");
+  if (srcbox.empty()) return fail(CGX_EINVAL, "transfer_data: empty srcbox");
+  for (int k = 0; k < 3; ++k)
+    if (dstbox.lo[k] < db.lo[k] || dstbox.up[k] > db.up[k] || dstbox.str[k] != db.str[k] ||
+        (dstbox.lo[k] - db.lo[k]) % dstbox.str[k])
+      return fail(CGX_EINVAL, "transfer_data: dstbox is not inside the destination");
+  int tl0, ntl, rc;
+  if ((rc = find_tl(times, nsrc, time, order_time, op, &tl0, &ntl))) return rc;
+  Built b;
+  memset(&b, 0, sizeof b);
+  Desc &d = b.d;
+  // with time interpolation the operator writes a temporary of extent
+  // dstbox (data.cc:506-509) and time_interpolate reads it with region
+  // dstbox (data.cc:517): the fused kernel writes dst directly
+  const Box &regdst = ntl > 1 ? dstbox : db;
+  if ((rc = build_spatial(op, cent, dst, &srcs[tl0], regdst, dstbox, srcbox, slab, order_space, &b)))
+    return rc;
+  int tk = T_NONE;
+  if (ntl > 1) {
+    const bool lagr = op == CGX_OP_COPY || op == CGX_OP_LAGRANGE;
+    const bool eno = op == CGX_OP_ENO || op == CGX_OP_WENO || op == CGX_OP_TVD ||
+                     op == CGX_OP_LAGRANGE_MONOTONE;
+    if (!lagr && !eno) return fail(CGX_EINVAL, "time_interpolate: bad operator");
+    if (order_time == 1) tk = T_LIN;
+    else if (order_time == 2) tk = lagr ? T_QUAD : T_ENO;
+    else return fail(CGX_EUNSUPPORTED, "time_interpolate: order_time %d is not provided", order_time);
+    if ((rc = time_weights(tk, times + tl0, time, d.w))) return rc;
+  }
+  d.ntl = ntl;
+  d.tkind = tk;
+  for (int t = 0; t < 3; ++t) d.src[t] = srcs[tl0 + std::min(t, ntl - 1)].data;
+  d.dst = dst->data;
+  d.dsy = dst->padext[0];
+  d.dsz = (long long)dst->padext[0] * dst->padext[1];
+  for (int k = 0; k < 3; ++k) d.doff[k] = (dstbox.lo[k] - db.lo[k]) / db.str[k];
+  // algorithmic bytes: destination written once, every timelevel's source
+  // read once (copy and restrictions counted per point above)
+  const long long src_bytes = b.bytes - 8 * b.points; // one timelevel's reads
+  b.bytes = 8 * b.points + (long long)ntl * src_bytes;
+  b.ntiles = kind_tiles(d.kind, d.n, d.tiles);
+  if (b.ntiles <= 0) return fail(CGX_EINVAL, "transfer: region too large");
+  *out = b;
+  return CGX_OK;
+}
+
+size_t smem_bytes_low() { return sizeof(double) * smem_doubles<5>(); }
+size_t smem_bytes_high() { return sizeof(double) * smem_doubles<11>(); }
+
+template <int FMA, bool HIGH> int ensure_pair_attr() {
+  if (!g_attr_done[FMA][HIGH]) {
+    cudaError_t e = cudaFuncSetAttribute(k_pair<FMA, HIGH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(HIGH ? smem_bytes_high() : smem_bytes_low()));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    g_attr_done[FMA][HIGH] = true;
+  }
+  return CGX_OK;
+}
+
+int launch_pair(const Desc &d, int ntiles, int fp, int *status, cudaStream_t s) {
+  const bool high = d.kind == K_PROLONG_VC && d.order >= 7;
+  int rc;
+  if (fp == CGX_FP_FMA) {
+    if (high) {
+      if ((rc = ensure_pair_attr<1, true>())) return rc;
+      k_pair<1, true><<<ntiles, NTHREADS, smem_bytes_high(), s>>>(d, status);
+    } else {
+      if ((rc = ensure_pair_attr<1, false>())) return rc;
+      k_pair<1, false><<<ntiles, NTHREADS, smem_bytes_low(), s>>>(d, status);
+    }
+  } else {
+    if (high) {
+      if ((rc = ensure_pair_attr<0, true>())) return rc;
+      k_pair<0, true><<<ntiles, NTHREADS, smem_bytes_high(), s>>>(d, status);
+    } else {
+      if ((rc = ensure_pair_attr<0, false>())) return rc;
+      k_pair<0, false><<<ntiles, NTHREADS, smem_bytes_low(), s>>>(d, status);
+    }
+  }
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? CGX_OK : cuda_fail(e, "kernel launch");
+}
+
+} // namespace
+
+// ============================================================== batches
+struct cgx_batch {
+  std::vector<Desc> descs;
+  std::vector<long long> bytes, points;
+  std::vector<int> ntiles;
+  std::vector<unsigned char> high; // vertex-centred orders 7..11: per-box kernels
+  Desc *d_descs = nullptr;
+  long long *d_prefix = nullptr;
+  size_t d_cap = 0;
+  int n_uploaded = 0;     // descriptors in the persistent kernel's queue
+  long long tiles_uploaded = 0;
+  std::vector<int> high_idx; // descriptors launched per box
+  unsigned long long *d_counter = nullptr;
+  int *d_status = nullptr;
+  int fp_mode = CGX_FP_EXACT;
+};
+
+struct cgx_graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" {
+
+const char *cgx_last_error(void) { return g_err.c_str(); }
+const char *cgx_version(void) { return "cgx 0.1 sm_100a fp64"; }
+
+int cgx_init(int device, int fp_mode) {
+  if (fp_mode != CGX_FP_EXACT && fp_mode != CGX_FP_FMA) return fail(CGX_EINVAL, "bad fp mode");
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  g_fp_mode = fp_mode;
+  return CGX_OK;
+}
+
+int cgx_set_fp_mode(int fp_mode) {
+  if (fp_mode != CGX_FP_EXACT && fp_mode != CGX_FP_FMA) return fail(CGX_EINVAL, "bad fp mode");
+  g_fp_mode = fp_mode;
+  return CGX_OK;
+}
+
+int cgx_find_source_timelevel(const double *times, int ntimes, double time, int order_time,
+                              int op, int *timelevel0, int *ntimelevels) {
+  return find_tl(times, ntimes, time, order_time, op, timelevel0, ntimelevels);
+}
+
+int cgx_transfer(int op, int cent, const cgx_array *dst, const cgx_array *srcs, const double *times,
+                 int nsrc, const int dstbox[9], const int srcbox[9], const int *slab_offset,
+                 double time, int order_space, int order_time, void *stream) {
+  Built b;
+  int rc = build(op, cent, dst, srcs, times, nsrc, dstbox, srcbox, slab_offset, time, order_space,
+                 order_time, &b);
+  if (rc) return rc;
+  return launch_pair(b.d, b.ntiles, g_fp_mode, nullptr, (cudaStream_t)stream);
+}
+
+int cgx_copy(int op, int cent, const cgx_array *dst, const cgx_array *src, const int dstbox[9],
+             const int srcbox[9], const int *slab_offset, void *stream) {
+  // gdata::copy_data, gdata.cc:110-122
+  const double t0 = 0.0;
+  return cgx_transfer(op, cent, dst, src, &t0, 1, dstbox, srcbox, slab_offset, 0.0,
+                      cent == CGX_VERTEX ? 1 : 0, 0, stream);
+}
+
+int cgx_batch_create(cgx_batch **out) {
+  if (!out) return fail(CGX_EINVAL, "null batch");
+  cgx_batch *b = new cgx_batch();
+  cudaError_t e = cudaMalloc(&b->d_counter, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_status, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(b->d_status, 0, sizeof(int));
+  if (e != cudaSuccess) {
+    cudaFree(b->d_counter);
+    delete b;
+    return cuda_fail(e, "cudaMalloc");
+  }
+  *out = b;
+  return CGX_OK;
+}
+
+int cgx_batch_destroy(cgx_batch *b) {
+  if (!b) return CGX_OK;
+  cudaFree(b->d_descs);
+  cudaFree(b->d_prefix);
+  cudaFree(b->d_counter);
+  cudaFree(b->d_status);
+  delete b;
+  return CGX_OK;
+}
+
+int cgx_batch_clear(cgx_batch *b) {
+  if (!b) return fail(CGX_EINVAL, "null batch");
+  b->descs.clear();
+  b->bytes.clear();
+  b->points.clear();
+  b->ntiles.clear();
+  b->high.clear();
+  return CGX_OK;
+}
+
+int cgx_batch_add(cgx_batch *b, int op, int cent, const cgx_array *dst, const cgx_array *srcs,
+                  const double *times, int nsrc, const int dstbox[9], const int srcbox[9],
+                  const int *slab_offset, double time, int order_space, int order_time) {
+  if (!b) return fail(CGX_EINVAL, "null batch");
+  Built x;
+  int rc = build(op, cent, dst, srcs, times, nsrc, dstbox, srcbox, slab_offset, time, order_space,
+                 order_time, &x);
+  if (rc) return rc;
+  b->descs.push_back(x.d);
+  b->bytes.push_back(x.bytes);
+  b->points.push_back(x.points);
+  b->ntiles.push_back(x.ntiles);
+  b->high.push_back(x.d.kind == K_PROLONG_VC && x.d.order >= 7);
+  return CGX_OK;
+}
+
+int cgx_batch_stats(const cgx_batch *b, int64_t *npairs, int64_t *ntiles, int64_t *dst_points,
+                    int64_t *bytes) {
+  if (!b) return fail(CGX_EINVAL, "null batch");
+  int64_t t = 0, p = 0, by = 0;
+  for (size_t i = 0; i < b->descs.size(); ++i) { t += b->ntiles[i]; p += b->points[i]; by += b->bytes[i]; }
+  if (npairs) *npairs = (int64_t)b->descs.size();
+  if (ntiles) *ntiles = t;
+  if (dst_points) *dst_points = p;
+  if (bytes) *bytes = by;
+  return CGX_OK;
+}
+
+int cgx_batch_upload(cgx_batch *b, void *stream) {
+  if (!b) return fail(CGX_EINVAL, "null batch");
+  cudaStream_t s = (cudaStream_t)stream;
+  // queue order: prolongation tiles (the heaviest) first, then the rest
+  std::vector<int> order;
+  b->high_idx.clear();
+  for (int pass = 0; pass < 2; ++pass)
+    for (size_t i = 0; i < b->descs.size(); ++i) {
+      if (b->high[i]) { if (pass == 0) b->high_idx.push_back((int)i); continue; }
+      bool prol = b->descs[i].kind >= K_PROLONG_VC;
+      if ((pass == 0) == prol) order.push_back((int)i);
+    }
+  const size_t n = order.size();
+  if (n > b->d_cap) {
+    cudaFree(b->d_descs);
+    cudaFree(b->d_prefix);
+    b->d_descs = nullptr;
+    b->d_prefix = nullptr;
+    size_t cap = std::max<size_t>(n, 64);
+    cudaError_t e = cudaMalloc(&b->d_descs, cap * sizeof(Desc));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_prefix, cap * sizeof(long long));
+    if (e != cudaSuccess) { b->d_cap = 0; return cuda_fail(e, "cudaMalloc"); }
+    b->d_cap = cap;
+  }
+  std::vector<Desc> hd(n);
+  std::vector<long long> hp(n);
+  long long acc = 0;
+  for (size_t i = 0; i < n; ++i) {
+    hd[i] = b->descs[order[i]];
+    hp[i] = acc;
+    acc += b->ntiles[order[i]];
+  }
+  b->n_uploaded = (int)n;
+  b->tiles_uploaded = acc;
+  b->fp_mode = g_fp_mode;
+  if (n) {
+    cudaError_t e = cudaMemcpyAsync(b->d_descs, hd.data(), n * sizeof(Desc), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(b->d_prefix, hp.data(), n * sizeof(long long), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s); // host vectors are temporaries
+    if (e != cudaSuccess) return cuda_fail(e, "descriptor upload");
+  }
+  return CGX_OK;
+}
+
+int cgx_batch_launch(cgx_batch *b, void *stream) {
+  if (!b) return fail(CGX_EINVAL, "null batch");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (b->n_uploaded > 0) {
+    cudaError_t e = cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int fp = b->fp_mode;
+    const size_t smem = smem_bytes_low();
+    if (!g_batch_attr_done[fp]) {
+      e = cudaFuncSetAttribute(fp ? k_batch<1> : k_batch<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+      g_batch_attr_done[fp] = true;
+    }
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fp ? k_batch<1> : k_batch<0>, NTHREADS, smem);
+    if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+    long long grid = std::min<long long>((long long)nsm * per_sm, b->tiles_uploaded);
+    if (fp) k_batch<1><<<(int)grid, NTHREADS, smem, s>>>(b->d_descs, b->d_prefix, b->n_uploaded,
+                                                          b->tiles_uploaded, b->d_counter, b->d_status);
+    else k_batch<0><<<(int)grid, NTHREADS, smem, s>>>(b->d_descs, b->d_prefix, b->n_uploaded,
+                                                       b->tiles_uploaded, b->d_counter, b->d_status);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "k_batch launch");
+  }
+  for (int i : b->high_idx) {
+    int rc = launch_pair(b->descs[i], b->ntiles[i], b->fp_mode, b->d_status, s);
+    if (rc) return rc;
+  }
+  return CGX_OK;
+}
+
+int cgx_batch_launch_per_box(cgx_batch *b, void *stream) {
+  if (!b) return fail(CGX_EINVAL, "null batch");
+  for (size_t i = 0; i < b->descs.size(); ++i) {
+    int rc = launch_pair(b->descs[i], b->ntiles[i], g_fp_mode, b->d_status, (cudaStream_t)stream);
+    if (rc) return rc;
+  }
+  return CGX_OK;
+}
+
+int cgx_batch_check(cgx_batch *b, void *stream) {
+  if (!b) return fail(CGX_EINVAL, "null batch");
+  int st = 0;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(&st, b->d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "status read");
+  if (st) {
+    cudaMemsetAsync(b->d_status, 0, sizeof(int), s);
+    return fail(st, "a kernel reported status %d", st);
+  }
+  return CGX_OK;
+}
+
+int cgx_graph_begin(void *stream) {
+  cudaError_t e = cudaStreamBeginCapture((cudaStream_t)stream, cudaStreamCaptureModeThreadLocal);
+  return e == cudaSuccess ? CGX_OK : cuda_fail(e, "cudaStreamBeginCapture");
+}
+
+int cgx_graph_end(void *stream, cgx_graph **out) {
+  if (!out) return fail(CGX_EINVAL, "null graph");
+  cgx_graph *g = new cgx_graph();
+  cudaError_t e = cudaStreamEndCapture((cudaStream_t)stream, &g->graph);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+  if (e != cudaSuccess) {
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return cuda_fail(e, "graph capture");
+  }
+  *out = g;
+  return CGX_OK;
+}
+
+int cgx_graph_launch(cgx_graph *g, void *stream) {
+  if (!g) return fail(CGX_EINVAL, "null graph");
+  cudaError_t e = cudaGraphLaunch(g->exec, (cudaStream_t)stream);
+  return e == cudaSuccess ? CGX_OK : cuda_fail(e, "cudaGraphLaunch");
+}
+
+int cgx_graph_destroy(cgx_graph *g) {
+  if (!g) return CGX_OK;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
+  return CGX_OK;
+}
+
+int cgx_malloc(void **ptr, size_t bytes) {
+  cudaError_t e = cudaMalloc(ptr, bytes);
+  return e == cudaSuccess ? CGX_OK : cuda_fail(e, "cudaMalloc");
+}
+int cgx_free(void *ptr) {
+  cudaError_t e = cudaFree(ptr);
+  return e == cudaSuccess ? CGX_OK : cuda_fail(e, "cudaFree");
+}
+int cgx_memcpy_htod(void *dst, const void *src, size_t bytes, void *stream) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream);
+  return e == cudaSuccess ? CGX_OK : cuda_fail(e, "cudaMemcpyAsync");
+}
+int cgx_memcpy_dtoh(void *dst, const void *src, size_t bytes, void *stream) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, (cudaStream_t)stream);
+  return e == cudaSuccess ? CGX_OK : cuda_fail(e, "cudaMemcpyAsync");
+}
+int cgx_stream_sync(void *stream) {
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  return e == cudaSuccess ? CGX_OK : cuda_fail(e, "cudaStreamSynchronize");
+}
+
+} // extern "C"

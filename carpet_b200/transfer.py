@@ -1,0 +1,193 @@
+"""Host-side mirror of CarpetLib's transfer interface.
+
+``Data`` stands for ``data<T>`` (CarpetLib/src/data.hh): the storage of one
+grid-function component at one timelevel, with its extent (a bbox) and
+padded shape, resident in device memory.  ``transfer_data`` and
+``copy_data`` take the arguments of ``gdata::transfer_data`` /
+``gdata::copy_data`` (CarpetLib/src/gdata.hh:182-191) for one process and
+call the C-ABI; errors that abort in CarpetLib raise ``CgxError`` here.
+
+``Batch`` collects many box-pairs (the ``sendrecv_pseudoregion`` walk of
+``ggf::transfer_from_all``, CarpetLib/src/ggf.cc:500-591) and runs them in
+one persistent kernel; ``Graph`` captures launches into a CUDA graph.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Sequence
+
+import torch
+
+from . import _lib
+from ._lib import CgxError, box9, check, cgx_array, ints3, lib
+
+# operator_type (CarpetLib/src/operators.hh:8-25), centering (defs.hh:134)
+OP_ERROR, OP_NONE, OP_SYNC, OP_RESTRICT, OP_COPY, OP_LAGRANGE, OP_ENO = range(7)
+VERTEX, CELL = 1, 2
+
+
+def set_fp_mode(fma: bool):
+    check(lib.cgx_set_fp_mode(_lib.FP_FMA if fma else _lib.FP_EXACT))
+
+
+def box_sizes(b: Sequence[int]):
+    return tuple(max(0, (b[3 + d] - b[d] + b[6 + d]) // b[6 + d]) for d in range(3))
+
+
+class Data:
+    """One component at one timelevel: a device array over ``extent``.
+
+    Stored as a float64 tensor of shape (padext_z, padext_y, padext_x); the x
+    extent is padded to an even number of elements so that every row starts
+    on a 16-byte boundary."""
+
+    def __init__(self, extent: Sequence[int], tensor: Optional[torch.Tensor] = None,
+                 device: str = "cuda"):
+        self.extent = [int(x) for x in extent]
+        nx, ny, nz = box_sizes(self.extent)
+        if tensor is None:
+            tensor = torch.empty((nz, ny, nx + (nx & 1)), dtype=torch.float64, device=device)
+        if tensor.dtype != torch.float64 or not tensor.is_contiguous() or tensor.dim() != 3:
+            raise ValueError("Data needs a contiguous 3-d float64 tensor")
+        pz, py, px = tensor.shape
+        if px < nx or py < ny or pz < nz:
+            raise ValueError("tensor smaller than the extent")
+        self.tensor = tensor
+
+    @property
+    def padext(self):
+        pz, py, px = self.tensor.shape
+        return (px, py, pz)
+
+    def cgx(self) -> cgx_array:
+        a = cgx_array()
+        a.data = self.tensor.data_ptr()
+        a.padext[:] = self.padext
+        a.bbox[:] = self.extent
+        return a
+
+
+def _stream(stream):
+    if stream is None:
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if isinstance(stream, torch.cuda.Stream):
+        return C.c_void_p(stream.cuda_stream)
+    return C.c_void_p(stream)
+
+
+def _arrays(srcs):
+    arr = (cgx_array * len(srcs))()
+    for i, s in enumerate(srcs):
+        arr[i] = s.cgx()
+    return arr
+
+
+def transfer_data(dst: Data, srcs: Sequence[Data], times: Sequence[float], dstbox, srcbox,
+                  time: float, order_space: int, order_time: int, op: int = OP_LAGRANGE,
+                  cent: int = VERTEX, slab_offset=None, stream=None):
+    """gdata::transfer_data for one box-pair on one process
+    (CarpetLib/src/gdata.cc:124-286): timelevel selection, spatial operator
+    per timelevel and time interpolation, fused in one launch."""
+    d = dst.cgx()
+    arr = _arrays(srcs)
+    ts = (C.c_double * len(times))(*times)
+    check(lib.cgx_transfer(op, cent, C.byref(d), arr, ts, len(srcs), box9(dstbox), box9(srcbox),
+                           ints3(slab_offset), float(time), int(order_space), int(order_time),
+                           _stream(stream)))
+
+
+def copy_data(dst: Data, src: Data, dstbox, srcbox, op: int = OP_LAGRANGE, cent: int = VERTEX,
+              slab_offset=None, stream=None):
+    """gdata::copy_data (CarpetLib/src/gdata.cc:110-122)."""
+    d, s = dst.cgx(), src.cgx()
+    check(lib.cgx_copy(op, cent, C.byref(d), C.byref(s), box9(dstbox), box9(srcbox),
+                       ints3(slab_offset), _stream(stream)))
+
+
+def find_source_timelevel(times, time, order_time, op):
+    tl0, ntl = C.c_int(), C.c_int()
+    ts = (C.c_double * len(times))(*times)
+    check(lib.cgx_find_source_timelevel(ts, len(times), float(time), int(order_time), int(op),
+                                        C.byref(tl0), C.byref(ntl)))
+    return tl0.value, ntl.value
+
+
+class Batch:
+    """Many box-pairs run by one persistent kernel."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        check(lib.cgx_batch_create(C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.cgx_batch_destroy(self.h)
+            self.h = None
+
+    def clear(self):
+        check(lib.cgx_batch_clear(self.h))
+
+    def add(self, dst: Data, srcs: Sequence[Data], times, dstbox, srcbox, time, order_space,
+            order_time, op=OP_LAGRANGE, cent=VERTEX, slab_offset=None):
+        d = dst.cgx()
+        arr = _arrays(srcs)
+        ts = (C.c_double * len(times))(*times)
+        check(lib.cgx_batch_add(self.h, op, cent, C.byref(d), arr, ts, len(srcs), box9(dstbox),
+                                box9(srcbox), ints3(slab_offset), float(time), int(order_space),
+                                int(order_time)))
+
+    def add_raw(self, op, cent, dst: cgx_array, srcs_arr, ts, nsrc, dstbox, srcbox, time,
+                order_space, order_time):
+        """add() for callers that already hold cgx_array structs"""
+        check(lib.cgx_batch_add(self.h, op, cent, C.byref(dst), srcs_arr, ts, nsrc, dstbox,
+                                srcbox, None, float(time), int(order_space), int(order_time)))
+
+    def stats(self):
+        v = [C.c_int64() for _ in range(4)]
+        check(lib.cgx_batch_stats(self.h, *[C.byref(x) for x in v]))
+        return dict(pairs=v[0].value, tiles=v[1].value, points=v[2].value, bytes=v[3].value)
+
+    def upload(self, stream=None):
+        check(lib.cgx_batch_upload(self.h, _stream(stream)))
+
+    def launch(self, stream=None):
+        check(lib.cgx_batch_launch(self.h, _stream(stream)))
+
+    def launch_per_box(self, stream=None):
+        check(lib.cgx_batch_launch_per_box(self.h, _stream(stream)))
+
+    def check(self, stream=None):
+        check(lib.cgx_batch_check(self.h, _stream(stream)))
+
+
+class Graph:
+    """CUDA graph of the calls made inside ``with g.capture(stream):``."""
+
+    def __init__(self):
+        self.h = None
+
+    class _Cap:
+        def __init__(self, g, stream):
+            self.g, self.s = g, stream
+
+        def __enter__(self):
+            check(lib.cgx_graph_begin(self.s))
+
+        def __exit__(self, et, ev, tb):
+            h = C.c_void_p()
+            rc = lib.cgx_graph_end(self.s, C.byref(h))
+            if et is None:
+                check(rc)
+                self.g.h = h
+
+    def capture(self, stream):
+        return Graph._Cap(self, _stream(stream))
+
+    def launch(self, stream=None):
+        check(lib.cgx_graph_launch(self.h, _stream(stream)))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.cgx_graph_destroy(self.h)
+            self.h = None

@@ -1,0 +1,158 @@
+/*
+ * cgx.h -- C-ABI of the B200 grid-transfer library (libcgx.so).
+ *
+ * Drop-in for the per-box-pair entry point of CarpetLib's transfer path:
+ * every grid function lives in device memory (HBM) of one GPU; the host
+ * passes device pointers, boxes and operator parameters, and the library
+ * launches hand-written sm_100a FP64 kernels.  No entry point aborts: each
+ * returns CGX_OK or a CGX_E* status; cgx_last_error() gives the message.
+ *
+ * Conventions shared with CarpetLib:
+ *   boxes   int[9] = {lower[3], upper[3], stride[3]}, inclusive bounds in the
+ *           global integer index space (bbox<int,3>, CarpetLib/src/bbox.hh:34-70;
+ *           the int[3][3] layout CarpetLib passes to Fortran, data.cc:212-214);
+ *   arrays  x-fastest, element (i,j,k) at i + padext[0]*(j + padext[1]*k)
+ *           (index3, CarpetLib/src/operator_prototypes_3d.hh:17-28); the logical
+ *           extent of an array is its bbox, padext[d] >= bbox size;
+ *   op      operator_type values of CarpetLib/src/operators.hh:8-25;
+ *   cent    centering values of CarpetLib/src/defs.hh:134.
+ */
+#ifndef CGX_H
+#define CGX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define CGX_OK 0
+#define CGX_EINVAL 1       /* inconsistent boxes/strides/times (CarpetLib aborts) */
+#define CGX_EUNSUPPORTED 2 /* operator/order not provided on the GPU */
+#define CGX_ENOMEM 3
+#define CGX_ECUDA 4        /* a CUDA runtime call failed */
+#define CGX_EDEVICE 5      /* a kernel reported a bad descriptor */
+
+/* operator_type, CarpetLib/src/operators.hh:8-25 */
+#define CGX_OP_ERROR 0
+#define CGX_OP_NONE 1
+#define CGX_OP_SYNC 2
+#define CGX_OP_RESTRICT 3
+#define CGX_OP_COPY 4
+#define CGX_OP_LAGRANGE 5
+#define CGX_OP_ENO 6
+#define CGX_OP_WENO 7
+#define CGX_OP_TVD 8
+#define CGX_OP_LAGRANGE_MONOTONE 9
+
+/* centering, CarpetLib/src/defs.hh:134 */
+#define CGX_VERTEX 1
+#define CGX_CELL 2
+
+/* floating-point modes of the stencil arithmetic */
+#define CGX_FP_EXACT 0 /* reference operation order, two roundings per
+                          multiply-add: bit-exact with CarpetLib built
+                          without contraction */
+#define CGX_FP_FMA 1   /* same order, every multiply-add fused */
+
+/* One device array of a grid function: one component at one timelevel.
+ * Mirrors what data<T> hands its operators: storage(), padded_shape(),
+ * extent() (CarpetLib/src/data.cc:610-614). */
+typedef struct cgx_array {
+  double *data;  /* device pointer */
+  int padext[3]; /* padded extent (x, y, z) in elements */
+  int bbox[9];   /* logical extent {lower[3], upper[3], stride[3]} */
+} cgx_array;
+
+/* Library state: floating-point mode and the default device. */
+int cgx_init(int device, int fp_mode);
+int cgx_set_fp_mode(int fp_mode);
+const char *cgx_last_error(void);
+const char *cgx_version(void);
+
+/*
+ * cgx_transfer -- the plain per-box form: one box-pair of
+ *   gdata::transfer_data(dst, state, srcs, times, dstbox, srcbox, slabinfo,
+ *                        dstproc, srcproc, time, order_space, order_time)
+ * (CarpetLib/src/gdata.hh:186-191, gdata.cc:124-286) on one process, i.e.
+ *   data<T>::transfer_from_innerloop (CarpetLib/src/data.cc:464-483).
+ * Same timelevel selection (gdata::find_source_timelevel, gdata.cc:288-349),
+ * same stride dispatch (transfer_p_r, data.cc:537-556), same operator tables
+ * (transfer_prolongate data.cc:573-725, transfer_restrict data.cc:1030-1135,
+ * time_interpolate data.cc:1183-1299), same argument checks as status codes.
+ * The spatial operator and the time interpolation run fused in one kernel,
+ * in the reference's order (space per timelevel, then time).
+ *   srcs[nsrc], times[nsrc]: source timelevels (same padext/bbox each);
+ *   slab_offset: NULL or int[3], the islab offset of copy_3d (copy_3d.cc:57);
+ *   stream: a cudaStream_t (NULL = default stream).
+ * Asynchronous: returns after the launch.
+ */
+int cgx_transfer(int op, int cent, const cgx_array *dst, const cgx_array *srcs,
+                 const double *times, int nsrc, const int dstbox[9],
+                 const int srcbox[9], const int *slab_offset, double time,
+                 int order_space, int order_time, void *stream);
+
+/* gdata::copy_data (CarpetLib/src/gdata.cc:110-122): transfer_data with
+ * order_space = (cent == vertex ? 1 : 0), order_time = 0, time 0. */
+int cgx_copy(int op, int cent, const cgx_array *dst, const cgx_array *src,
+             const int dstbox[9], const int srcbox[9], const int *slab_offset,
+             void *stream);
+
+/* The timelevel selection alone (gdata::find_source_timelevel). */
+int cgx_find_source_timelevel(const double *times, int ntimes, double time,
+                              int order_time, int op, int *timelevel0,
+                              int *ntimelevels);
+
+/*
+ * Batched form: many box-pairs -- of one refinement level or of several
+ * hierarchies, uneven sizes, mixed operators -- validated once on the host
+ * into flat descriptors, then run by one persistent kernel that takes tiles
+ * from a device work queue.  Replaces the loop of ggf::transfer_from_all
+ * (CarpetLib/src/ggf.cc:500-591) over a sendrecv_pseudoregion list.
+ */
+typedef struct cgx_batch cgx_batch;
+int cgx_batch_create(cgx_batch **out);
+int cgx_batch_destroy(cgx_batch *b);
+int cgx_batch_clear(cgx_batch *b);
+/* same arguments and checks as cgx_transfer; appends one box-pair */
+int cgx_batch_add(cgx_batch *b, int op, int cent, const cgx_array *dst,
+                  const cgx_array *srcs, const double *times, int nsrc,
+                  const int dstbox[9], const int srcbox[9],
+                  const int *slab_offset, double time, int order_space,
+                  int order_time);
+/* number of box-pairs, tiles and algorithmic bytes (reads + writes) */
+int cgx_batch_stats(const cgx_batch *b, int64_t *npairs, int64_t *ntiles,
+                    int64_t *dst_points, int64_t *bytes);
+/* copy descriptors to the device (once per schedule; graph-safe after) */
+int cgx_batch_upload(cgx_batch *b, void *stream);
+/* one persistent-kernel launch over every uploaded box-pair */
+int cgx_batch_launch(cgx_batch *b, void *stream);
+/* plain per-box launches of the same descriptors (one kernel per pair) */
+int cgx_batch_launch_per_box(cgx_batch *b, void *stream);
+/* device status word of the last launches: 0 or a CGX_E* code */
+int cgx_batch_check(cgx_batch *b, void *stream);
+
+/*
+ * CUDA graphs: capture a sequence of batch launches (a Berger-Oliger
+ * substep) once and replay it.  Begin/end bracket ordinary calls on
+ * `stream`.
+ */
+typedef struct cgx_graph cgx_graph;
+int cgx_graph_begin(void *stream);
+int cgx_graph_end(void *stream, cgx_graph **out);
+int cgx_graph_launch(cgx_graph *g, void *stream);
+int cgx_graph_destroy(cgx_graph *g);
+
+/* device memory helpers for callers without their own allocator */
+int cgx_malloc(void **ptr, size_t bytes);
+int cgx_free(void *ptr);
+int cgx_memcpy_htod(void *dst, const void *src, size_t bytes, void *stream);
+int cgx_memcpy_dtoh(void *dst, const void *src, size_t bytes, void *stream);
+int cgx_stream_sync(void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CGX_H */

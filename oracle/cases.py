@@ -149,7 +149,7 @@ def copy_case(rng, stride=1, max_ext=9, slab=False, kind="normal"):
     src = _fill(rng, alloc(srcbbox), kind)
     dst = alloc(dstbbox, fill=np.nan)
     return dict(src=src, srcbbox=srcbbox, dst=dst, dstbbox=dstbbox,
-                srcreg=srcreg if slab else dstreg, dstreg=dstreg,
+                srcreg=srcreg if slab else dstreg, dstreg=dstreg, reg=dstreg,
                 slab=[int(x) for x in off] if slab else None)
 
 

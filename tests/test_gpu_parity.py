@@ -1,0 +1,226 @@
+"""GPU parity: the sm_100a kernels through the C-ABI against the oracle.
+
+Every case runs the same seeded inputs through ``cgx_transfer`` (and the
+batched persistent kernel) and through the oracle's restatement of
+``gdata::transfer_data`` (oracle/cgx_oracle.c), in the same floating-point
+mode.  The bar is bit-exact: whole destination arrays are compared as bit
+patterns, so values outside the region (NaN-filled) must stay untouched.
+In the exact mode the oracle is itself bit-exact with CarpetLib's own
+operators (tests/test_oracle.py), and so, transitively, is the GPU.
+"""
+import numpy as np
+import pytest
+
+from oracle import cases
+from oracle.binding import OP_COPY, OP_ENO, OP_LAGRANGE, CELL, VERTEX
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def cgx():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import carpet_b200 as cb
+    return cb
+
+
+def bits_equal(a, b):
+    return np.array_equal(np.ascontiguousarray(a).view(np.uint64),
+                          np.ascontiguousarray(b).view(np.uint64))
+
+
+def to_dev(cb, a, bbox):
+    return cb.Data(bbox, torch.from_numpy(a.copy()).cuda())
+
+
+def timeset(rng, ntl):
+    """(times, time, order_time) that select ntl timelevels"""
+    t0, dt = float(rng.uniform(-1, 1)), float(rng.uniform(0.05, 0.5))
+    times = [t0, t0 - dt, t0 - 2 * dt]
+    if ntl == 1:
+        return times, times[int(rng.integers(0, 3))], 2
+    lo = times[ntl - 1]  # 2 timelevels interpolate between TL0 and TL1
+    return times, float(rng.uniform(lo + 1e-3, times[0] - 1e-3)), ntl - 1
+
+
+def run_pair(cb, port, c, op, cent, order, ntl, fma, rng, batch=False):
+    times, time, ot = timeset(rng, ntl)
+    srcs_np = [c["src"], c["src"] * 0.5 + 0.25, c["src"] * -1.5 + 1.0]
+    want = c["dst"].copy()
+    port.transfer(op, cent, want, c["dstbbox"], srcs_np, c["srcbbox"], times, c["reg"],
+                  c["srcbbox"], time, order, ot, fma=fma)
+    dst = to_dev(cb, c["dst"], c["dstbbox"])
+    srcs = [to_dev(cb, s, c["srcbbox"]) for s in srcs_np]
+    cb.set_fp_mode(fma)
+    if batch:
+        b = cb.Batch()
+        b.add(dst, srcs, times, c["reg"], c["srcbbox"], time, order, ot, op=op, cent=cent)
+        b.upload()
+        b.launch()
+        b.check()
+    else:
+        cb.transfer_data(dst, srcs, times, c["reg"], c["srcbbox"], time, order, ot, op=op,
+                         cent=cent)
+    torch.cuda.synchronize()
+    got = dst.tensor.cpu().numpy()
+    return got, want
+
+
+@pytest.mark.parametrize("fma", [False, True], ids=["exact", "fma"])
+@pytest.mark.parametrize("ntl", [1, 2, 3])
+@pytest.mark.parametrize("order", [1, 3, 5, 7, 9, 11])
+def test_vc_lagrange(cgx, port, order, ntl, fma):
+    rng = np.random.default_rng(1000 + 10 * order + ntl)
+    for it in range(6):
+        big = it >= 4
+        c = cases.vc_prolong_case(rng, order, fine_stride=int(rng.choice([1, 2])),
+                                  max_ext=40 if big else 9,
+                                  kind=("normal", "mixed")[it % 2])
+        got, want = run_pair(cgx, port, c, OP_LAGRANGE, VERTEX, order, ntl, fma, rng)
+        assert bits_equal(got, want), np.nanmax(np.abs(got - want))
+
+
+@pytest.mark.parametrize("fma", [False, True], ids=["exact", "fma"])
+@pytest.mark.parametrize("ntl", [1, 2, 3])
+@pytest.mark.parametrize("order", [0, 1, 2, 3, 4, 5])
+def test_cc_lagrange(cgx, port, order, ntl, fma):
+    rng = np.random.default_rng(2000 + 10 * order + ntl)
+    for it in range(5):
+        c = cases.cc_prolong_case(rng, order, half=int(rng.choice([1, 2])),
+                                  max_ext=36 if it == 4 else 9,
+                                  kind=("normal", "mixed")[it % 2])
+        got, want = run_pair(cgx, port, c, OP_LAGRANGE, CELL, order, ntl, fma, rng)
+        assert bits_equal(got, want)
+
+
+@pytest.mark.parametrize("fma", [False, True], ids=["exact", "fma"])
+@pytest.mark.parametrize("ntl", [1, 2, 3])
+def test_vc_eno(cgx, port, ntl, fma):
+    rng = np.random.default_rng(3000 + ntl)
+    for it in range(8):
+        c = cases.vc_prolong_case(rng, 3, reach=(1, 2), max_ext=40 if it == 7 else 9,
+                                  kind=("normal", "steps", "mixed")[it % 3])
+        got, want = run_pair(cgx, port, c, OP_ENO, VERTEX, 3, ntl, fma, rng)
+        assert bits_equal(got, want)
+
+
+@pytest.mark.parametrize("fma", [False, True], ids=["exact", "fma"])
+def test_restrict_and_copy(cgx, port, fma):
+    rng = np.random.default_rng(4000)
+    for it in range(10):
+        big = it == 9
+        for maker, cent in ((cases.vc_restrict_case, VERTEX), (cases.cc_restrict_case, CELL)):
+            c = maker(rng, max_ext=40 if big else 9, kind="mixed")
+            got, want = run_pair(cgx, port, c, OP_LAGRANGE, cent, 1, 1, fma, rng)
+            assert bits_equal(got, want)
+        c = cases.copy_case(rng, max_ext=40 if big else 9, kind="mixed")
+        for ntl in (1, 2, 3):
+            got, want = run_pair(cgx, port, c, OP_LAGRANGE, VERTEX, 1, ntl, fma, rng)
+            assert bits_equal(got, want)
+
+
+def test_copy_with_slab_offset(cgx, port):
+    rng = np.random.default_rng(4100)
+    for it in range(10):
+        c = cases.copy_case(rng, slab=True, kind="mixed")
+        want = c["dst"].copy()
+        port.copy_3d(c["src"], c["srcbbox"], want, c["dstbbox"], c["srcreg"], c["dstreg"], c["slab"])
+        dst = to_dev(cgx, c["dst"], c["dstbbox"])
+        src = to_dev(cgx, c["src"], c["srcbbox"])
+        cgx.copy_data(dst, src, c["dstreg"], c["srcreg"], slab_offset=c["slab"])
+        torch.cuda.synchronize()
+        assert bits_equal(dst.tensor.cpu().numpy(), want)
+
+
+@pytest.mark.parametrize("fma", [False, True], ids=["exact", "fma"])
+def test_batched_mixed_pairs_match_per_box_and_oracle(cgx, port, fma):
+    """A batch of uneven, mixed box-pairs (each with its own destination)
+    in one persistent kernel, then the same descriptors per box, then a
+    CUDA-graph replay: all three bit-identical with the oracle."""
+    rng = np.random.default_rng(5000)
+    cgx.set_fp_mode(fma)
+    b = cgx.Batch()
+    items = []
+    for it in range(60):
+        kind = it % 6
+        ntl = int(rng.integers(1, 4))
+        if kind == 0:
+            order = int(rng.choice([1, 3, 5]))
+            c = cases.vc_prolong_case(rng, order, max_ext=int(rng.integers(3, 40)))
+            op, cent = OP_LAGRANGE, VERTEX
+        elif kind == 1:
+            order = int(rng.integers(0, 6))
+            c = cases.cc_prolong_case(rng, order, max_ext=int(rng.integers(3, 30)))
+            op, cent = OP_LAGRANGE, CELL
+        elif kind == 2:
+            order = 3
+            c = cases.vc_prolong_case(rng, 3, reach=(1, 2), max_ext=int(rng.integers(3, 30)))
+            op, cent = OP_ENO, VERTEX
+        elif kind == 3:
+            order, op, cent = 1, OP_LAGRANGE, VERTEX
+            c = cases.vc_restrict_case(rng, max_ext=int(rng.integers(3, 30)))
+            ntl = 1
+        elif kind == 4:
+            order, op, cent = 0, OP_LAGRANGE, CELL
+            c = cases.cc_restrict_case(rng, max_ext=int(rng.integers(3, 30)))
+            ntl = 1
+        else:
+            order, op, cent = 1, OP_LAGRANGE, VERTEX
+            c = cases.copy_case(rng, max_ext=int(rng.integers(3, 40)))
+        times, time, ot = timeset(rng, ntl)
+        srcs_np = [c["src"], c["src"] * 0.5 + 0.25, c["src"] * -1.5 + 1.0]
+        want = c["dst"].copy()
+        port.transfer(op, cent, want, c["dstbbox"], srcs_np, c["srcbbox"], times, c["reg"]
+                      if "reg" in c else c["dstreg"], c["srcbbox"], time, order, ot, fma=fma)
+        dst = to_dev(cgx, c["dst"], c["dstbbox"])
+        srcs = [to_dev(cgx, s, c["srcbbox"]) for s in srcs_np]
+        b.add(dst, srcs, times, c["reg"] if "reg" in c else c["dstreg"], c["srcbbox"], time,
+              order, ot, op=op, cent=cent)
+        items.append((dst, srcs, want, c["dst"]))
+    st = b.stats()
+    assert st["pairs"] == 60 and st["tiles"] > 60
+    b.upload()
+    for mode in ("batch", "per_box", "graph"):
+        for dst, _, _, init in items:
+            dst.tensor.copy_(torch.from_numpy(init))
+        if mode == "batch":
+            b.launch()
+        elif mode == "per_box":
+            b.launch_per_box()
+        else:
+            s = torch.cuda.Stream()
+            g = cgx.Graph()
+            torch.cuda.synchronize()
+            with g.capture(s):
+                b.launch(s)
+            g.launch(s)
+            g.launch(s)
+            s.synchronize()
+        b.check()
+        torch.cuda.synchronize()
+        for dst, _, want, _ in items:
+            assert bits_equal(dst.tensor.cpu().numpy(), want), mode
+
+
+def test_exact_mode_matches_compiled_reference(cgx):
+    """Directly against CarpetLib's operators compiled from source, where
+    that build travelled with the tree."""
+    from oracle.binding import Ref
+    if not Ref.available():
+        pytest.skip("reference build absent")
+    ref = Ref(False)
+    rng = np.random.default_rng(6000)
+    cgx.set_fp_mode(False)
+    for order in (1, 3, 5):
+        for it in range(4):
+            c = cases.vc_prolong_case(rng, order, max_ext=30, kind="mixed")
+            want = c["dst"].copy()
+            ref.prolongate_3d_rf2(order, c["src"], c["srcbbox"], want, c["dstbbox"], c["reg"])
+            dst = to_dev(cgx, c["dst"], c["dstbbox"])
+            src = to_dev(cgx, c["src"], c["srcbbox"])
+            cgx.transfer_data(dst, [src], [0.0], c["reg"], c["srcbbox"], 0.0, order, 0)
+            torch.cuda.synchronize()
+            assert bits_equal(dst.tensor.cpu().numpy(), want)
