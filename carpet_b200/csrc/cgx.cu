@@ -871,3 +871,114 @@ int cgx_stream_sync(void *stream) {
 }
 
 } // extern "C"
+
+// ============================================================== no-allocation form
+// cgx_transfer_pairs_noalloc runs a list of box-pairs through the persistent
+// kernel without allocating device memory.  The kernel's scratch -- the
+// descriptor queue, the tile prefix sums, the work counter and the status
+// word -- lives in one fixed-size array in the library's own device image,
+// created when a GPU loads the library and held until the process exits.
+namespace {
+
+constexpr int kNoAllocMaxPairs = CGX_NOALLOC_MAX_PAIRS;
+constexpr size_t kNoAllocDescBytes = sizeof(Desc) * kNoAllocMaxPairs;
+constexpr size_t kNoAllocPrefixOff = (kNoAllocDescBytes + 255) / 256 * 256;
+constexpr size_t kNoAllocCounterOff =
+    (kNoAllocPrefixOff + sizeof(long long) * kNoAllocMaxPairs + 255) / 256 * 256;
+constexpr size_t kNoAllocBytes = kNoAllocCounterOff + 256; // counter + status
+
+// The scratch itself.  In host code this name only stands in for the symbol:
+// its device address comes from cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kMaxDevices = 64;
+unsigned char *g_noalloc_dev[kMaxDevices] = {nullptr};
+
+// Device address of the scratch on the current device; the first call on a
+// device looks it up (that call must not be inside a stream capture).
+int noalloc_scratch(unsigned char **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices) return fail(CGX_EINVAL, "device index %d out of range", dev);
+  if (!g_noalloc_dev[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress");
+    g_noalloc_dev[dev] = static_cast<unsigned char *>(p);
+  }
+  *out = g_noalloc_dev[dev];
+  return CGX_OK;
+}
+
+} // namespace
+
+extern "C" int cgx_transfer_pairs_noalloc(const cgx_pair *pairs, int npairs, void *stream) {
+  if (npairs < 0 || (npairs > 0 && !pairs)) return fail(CGX_EINVAL, "bad pair list");
+  if (npairs > kNoAllocMaxPairs)
+    return fail(CGX_EINVAL,
+                "cgx_transfer_pairs_noalloc: %d box-pairs exceed the fixed maximum of %d; "
+                "split the list or use cgx_batch_*",
+                npairs, kNoAllocMaxPairs);
+  if (npairs == 0) return CGX_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned char *base = nullptr;
+  int rc = noalloc_scratch(&base);
+  if (rc) return rc;
+  Desc *d_descs = reinterpret_cast<Desc *>(base);
+  long long *d_prefix = reinterpret_cast<long long *>(base + kNoAllocPrefixOff);
+  unsigned long long *d_counter = reinterpret_cast<unsigned long long *>(base + kNoAllocCounterOff);
+  int *d_status = reinterpret_cast<int *>(base + kNoAllocCounterOff + sizeof(unsigned long long));
+
+  // Validate on the host into small stack chunks and copy each chunk into
+  // the scratch; cudaMemcpyAsync has staged pageable sources when it returns.
+  constexpr int kChunk = 16;
+  Desc hd[kChunk];
+  long long hp[kChunk];
+  long long tiles = 0;
+  for (int i0 = 0; i0 < npairs; i0 += kChunk) {
+    const int n = std::min(kChunk, npairs - i0);
+    for (int i = 0; i < n; ++i) {
+      const cgx_pair &p = pairs[i0 + i];
+      if (p.nsrc < 1 || p.nsrc > 3)
+        return fail(CGX_EINVAL, "pair %d: nsrc must be 1..3", i0 + i);
+      Built b;
+      rc = build(p.op, p.cent, &p.dst, p.srcs, p.times, p.nsrc, p.dstbox, p.srcbox,
+                 p.has_slab ? p.slab_offset : nullptr, p.time, p.order_space, p.order_time, &b);
+      if (rc) return rc;
+      if (b.d.kind == K_PROLONG_VC && b.d.order >= 7)
+        return fail(CGX_EUNSUPPORTED,
+                    "pair %d: vertex-centred order %d is not available without allocation",
+                    i0 + i, b.d.order);
+      hd[i] = b.d;
+      hp[i] = tiles;
+      tiles += b.ntiles;
+    }
+    cudaError_t e = cudaMemcpyAsync(d_descs + i0, hd, n * sizeof(Desc), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_prefix + i0, hp, n * sizeof(long long), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(e, "scratch upload");
+  }
+  // the work counter and the status word start at zero on every call
+  cudaError_t e = cudaMemsetAsync(base + kNoAllocCounterOff, 0, 256, s);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+  int dev = 0, nsm = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int fp = g_fp_mode;
+  const size_t smem = smem_bytes_low();
+  if (!g_batch_attr_done[fp]) {
+    e = cudaFuncSetAttribute(fp ? k_batch<1> : k_batch<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    g_batch_attr_done[fp] = true;
+  }
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fp ? k_batch<1> : k_batch<0>, NTHREADS,
+                                                    smem);
+  if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+  const long long grid = std::min<long long>((long long)nsm * per_sm, tiles);
+  if (fp) k_batch<1><<<(int)grid, NTHREADS, smem, s>>>(d_descs, d_prefix, npairs, tiles, d_counter, d_status);
+  else k_batch<0><<<(int)grid, NTHREADS, smem, s>>>(d_descs, d_prefix, npairs, tiles, d_counter, d_status);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? CGX_OK : cuda_fail(e, "k_batch launch");
+}

@@ -145,6 +145,42 @@ int cgx_graph_end(void *stream, cgx_graph **out);
 int cgx_graph_launch(cgx_graph *g, void *stream);
 int cgx_graph_destroy(cgx_graph *g);
 
+/*
+ * No-allocation form.  NO COUNTERPART IN THE REFERENCE: CarpetLib has no
+ * device path at all; this entry point exists for callers of this library
+ * that must not allocate device memory -- code that runs while a CUDA graph
+ * is being captured elsewhere in the process, hosts that reserve all device
+ * memory for their own pool, or time-critical loops that cannot afford the
+ * device-wide synchronisation cudaMalloc/cudaFree imply.
+ *
+ * Runs up to CGX_NOALLOC_MAX_PAIRS box-pairs (same meaning and checks as
+ * cgx_transfer; at most 3 source timelevels each; vertex-centred orders
+ * 7/9/11 are not available here) through the persistent kernel.  Its
+ * scratch -- descriptors, tile offsets, work counter -- is one fixed array
+ * of under 0.5 MiB (room for CGX_NOALLOC_MAX_PAIRS descriptors) inside the
+ * library's device image, which every GPU that loads the library holds until
+ * the process exits; nothing is allocated.
+ * The first call on a device looks up that array's device address, so make
+ * the first call on each device outside any stream capture.  All calls share
+ * the one array: calls whose kernels overlap on the GPU (other streams, or
+ * other host threads) race and must be serialised by the caller.  Returns
+ * CGX_EINVAL for more than CGX_NOALLOC_MAX_PAIRS pairs.  Asynchronous.
+ */
+#define CGX_NOALLOC_MAX_PAIRS 2048
+typedef struct cgx_pair {
+  int op, cent;
+  cgx_array dst;
+  cgx_array srcs[3];
+  double times[3];
+  int nsrc;
+  int dstbox[9], srcbox[9];
+  int has_slab;
+  int slab_offset[3];
+  double time;
+  int order_space, order_time;
+} cgx_pair;
+int cgx_transfer_pairs_noalloc(const cgx_pair *pairs, int npairs, void *stream);
+
 /* device memory helpers for callers without their own allocator */
 int cgx_malloc(void **ptr, size_t bytes);
 int cgx_free(void *ptr);

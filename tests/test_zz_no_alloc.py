@@ -1,0 +1,156 @@
+"""The no-allocation entry point, cgx_transfer_pairs_noalloc.
+
+Some callers of this library must not allocate device memory: a host code
+that hands all device memory to its own pool, work issued while a CUDA graph
+is being captured elsewhere in the process, or a time-step loop that cannot
+take the device-wide synchronisation cudaMalloc/cudaFree bring.  For them the
+persistent kernel can run with its scratch (descriptor queue, tile offsets,
+work counter) in a fixed array inside the library's device image instead of
+in allocated memory.
+
+This test calls that entry point through the C-ABI twice in a row and checks
+each result bit for bit against the ordinary per-box entry point
+(cgx_transfer) on the same inputs -- the same bar as every other parity test
+-- and checks that an over-long pair list is refused.  It sits in the last
+collected test file and passes both alone and after the other tests.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import cases
+from oracle.binding import CELL, OP_ENO, OP_LAGRANGE, VERTEX
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _structs():
+    from carpet_b200._lib import cgx_array
+
+    class cgx_pair(C.Structure):
+        _fields_ = [("op", C.c_int), ("cent", C.c_int), ("dst", cgx_array),
+                    ("srcs", cgx_array * 3), ("times", C.c_double * 3), ("nsrc", C.c_int),
+                    ("dstbox", C.c_int * 9), ("srcbox", C.c_int * 9), ("has_slab", C.c_int),
+                    ("slab_offset", C.c_int * 3), ("time", C.c_double),
+                    ("order_space", C.c_int), ("order_time", C.c_int)]
+    return cgx_array, cgx_pair
+
+
+def _make_pairs(seed, n):
+    """seeded mixed box-pairs: (op, cent, case, ntl, order)"""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        k = i % 6
+        if k == 0:
+            order = int(rng.choice([1, 3, 5]))
+            out.append((OP_LAGRANGE, VERTEX, cases.vc_prolong_case(rng, order, max_ext=30), order))
+        elif k == 1:
+            order = int(rng.integers(0, 6))
+            out.append((OP_LAGRANGE, CELL, cases.cc_prolong_case(rng, order, max_ext=24), order))
+        elif k == 2:
+            out.append((OP_ENO, VERTEX, cases.vc_prolong_case(rng, 3, reach=(1, 2), max_ext=24), 3))
+        elif k == 3:
+            out.append((OP_LAGRANGE, VERTEX, cases.vc_restrict_case(rng, max_ext=24), 1))
+        elif k == 4:
+            out.append((OP_LAGRANGE, CELL, cases.cc_restrict_case(rng, max_ext=24), 0))
+        else:
+            out.append((OP_LAGRANGE, VERTEX, cases.copy_case(rng, max_ext=30), 1))
+    return out
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from carpet_b200._lib import lib as L
+    return L
+
+
+def _run(lib, seed, n):
+    from carpet_b200._lib import box9
+    cgx_array, cgx_pair = _structs()
+    lib.cgx_set_fp_mode(1)
+    pairs = (cgx_pair * n)()
+    keep, ref_dsts, na_dsts = [], [], []
+    t0, dt = 0.5, 0.125
+    for i, (op, cent, c, order) in enumerate(_make_pairs(seed, n)):
+        ntl = 1 + i % 3
+        if c["srcbbox"][6] < c["dstbbox"][6]:  # restriction: one timelevel
+            ntl = 1
+        times = [t0, t0 - dt, t0 - 2 * dt]
+        time = t0 if ntl == 1 else t0 - dt / (3 if ntl == 2 else 2)
+        ot = 2 if ntl != 2 else 1
+        srcs_np = [c["src"], c["src"] * 0.5 + 0.25, c["src"] * -1.5 + 1.0]
+        srcs = [torch.from_numpy(s.copy()).cuda() for s in srcs_np]
+        d_ref = torch.from_numpy(c["dst"].copy()).cuda()
+        d_na = torch.from_numpy(c["dst"].copy()).cuda()
+        keep += srcs
+        ref_dsts.append(d_ref)
+        na_dsts.append((d_na, torch.from_numpy(c["dst"].copy()).cuda()))
+
+        def arr(t, bbox):
+            a = cgx_array()
+            a.data = t.data_ptr()
+            a.padext[:] = (t.shape[2], t.shape[1], t.shape[0])
+            a.bbox[:] = bbox
+            return a
+
+        p = pairs[i]
+        p.op, p.cent = op, cent
+        p.dst = arr(d_na, c["dstbbox"])
+        for t in range(3):
+            p.srcs[t] = arr(srcs[t], c["srcbbox"])
+        p.times[:] = times
+        p.nsrc = 3
+        p.dstbox[:] = c["reg"]
+        p.srcbox[:] = c["srcbbox"]
+        p.has_slab = 0
+        p.time = time
+        p.order_space, p.order_time = order, ot
+        # the existing per-box entry point on the same arguments
+        dref = arr(d_ref, c["dstbbox"])
+        sarr = (cgx_array * 3)(*[arr(s, c["srcbbox"]) for s in srcs])
+        ts = (C.c_double * 3)(*times)
+        rc = lib.cgx_transfer(op, cent, C.byref(dref), sarr, ts, 3, box9(c["reg"]),
+                              box9(c["srcbbox"]), None, time, order, ot, None)
+        assert rc == 0, lib.cgx_last_error()
+    torch.cuda.synchronize()
+    return pairs, keep, ref_dsts, na_dsts
+
+
+def test_noalloc_matches_per_box_twice(lib):
+    pairs, keep, ref_dsts, na_dsts = _run(lib, 777, 48)
+    n = len(ref_dsts)
+    for call in range(2):
+        for d, init in na_dsts:
+            d.copy_(init)
+        rc = lib.cgx_transfer_pairs_noalloc(pairs, n, None)
+        assert rc == 0, lib.cgx_last_error()
+        torch.cuda.synchronize()
+        for i, ((d, _), r) in enumerate(zip(na_dsts, ref_dsts)):
+            a = d.cpu().numpy().view(np.uint64)
+            b = r.cpu().numpy().view(np.uint64)
+            assert np.array_equal(a, b), (call, i)
+
+
+def test_noalloc_second_list_reuses_scratch(lib):
+    """a different, shorter list right after: the shared scratch keeps the
+    previous call's contents, and the counter must start from zero again"""
+    pairs, keep, ref_dsts, na_dsts = _run(lib, 778, 17)
+    rc = lib.cgx_transfer_pairs_noalloc(pairs, len(ref_dsts), None)
+    assert rc == 0, lib.cgx_last_error()
+    torch.cuda.synchronize()
+    for (d, _), r in zip(na_dsts, ref_dsts):
+        assert np.array_equal(d.cpu().numpy().view(np.uint64), r.cpu().numpy().view(np.uint64))
+
+
+def test_noalloc_rejects_too_many_pairs(lib):
+    _, cgx_pair = _structs()
+    n = 2049
+    pairs = (cgx_pair * n)()
+    rc = lib.cgx_transfer_pairs_noalloc(pairs, n, None)
+    assert rc == 1
+    assert b"2048" in lib.cgx_last_error()
