@@ -40,6 +40,18 @@ def _padded(ext_box):
     return nx + (nx & 1), ny, nz
 
 
+def storage_bytes(h: Hierarchy, ngf: int, ntl: int) -> int:
+    """device bytes a Storage of this hierarchy allocates"""
+    n = 0
+    for lev in h.levels:
+        per = 0
+        for c in lev.comps:
+            px, py, pz = _padded(c.exterior)
+            per += ((px * py * pz + 31) // 32) * 32
+        n += ntl * ngf * per * 8
+    return n
+
+
 class Storage:
     """[level][tl] -> one pool; data[level][tl][gf][comp] -> Data views"""
 

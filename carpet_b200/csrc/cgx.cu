@@ -7,10 +7,8 @@
 // and turns one box-pair into one device descriptor (cgx::Desc).  The
 // reference aborts on bad arguments; here every check returns a status.
 //
-// Device side: cgx_device.cuh.  Two kernels run the same tile routines:
-//   k_pair   grid = the tiles of one descriptor (the plain per-box form);
-//   k_batch  persistent, one CTA per SM slot, tiles of many descriptors
-//            taken from a device work counter.
+// Device side: cgx_device.cuh (tile routines) and cgx_kernels.cuh
+// (kernels), launched through cgx_kern_*.cu.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -23,130 +21,15 @@
 
 #include "../../include/cgx.h"
 #include "cgx_device.cuh"
+#include "cgx_internal.h"
 
 using namespace cgx;
-
-// ============================================================== device side
-namespace {
-
-__device__ __forceinline__ void report(int *status, int code) {
-  if (status) atomicCAS(status, 0, code);
-}
-
-// dynamic shared memory of the largest variant a kernel dispatches
-template <int MAXORDER> constexpr int smem_doubles() {
-  return PSmem<VC<MAXORDER>, 3>::total > PSmem<CC<5>, 3>::total
-             ? PSmem<VC<MAXORDER>, 3>::total
-             : PSmem<CC<5>, 3>::total;
-}
-
-template <class F, int FMA>
-__device__ __forceinline__ void prolong_ntl(const Desc &d, int tile, double *sm) {
-  switch (d.ntl) {
-  case 1: prolong_tile<F, FMA, 1, T_NONE>(d, tile, sm); break;
-  case 2: prolong_tile<F, FMA, 2, T_LIN>(d, tile, sm); break;
-  default:
-    if (d.tkind == T_ENO) prolong_tile<F, FMA, 3, T_ENO>(d, tile, sm);
-    else prolong_tile<F, FMA, 3, T_QUAD>(d, tile, sm);
-  }
-}
-
-// HIGH selects the vertex-centred orders 7/9/11, which live in their own
-// kernel so that their larger register windows do not lower the occupancy
-// of the common orders.
-template <int FMA, bool HIGH>
-__device__ __forceinline__ void run_tile(const Desc &d, int tile, double *sm, int *status) {
-  switch (d.kind) {
-  case K_COPY:
-    if (d.ntl == 1) copy_tile<FMA, 1, T_NONE>(d, tile);
-    else if (d.ntl == 2) copy_tile<FMA, 2, T_LIN>(d, tile);
-    else if (d.tkind == T_ENO) copy_tile<FMA, 3, T_ENO>(d, tile);
-    else copy_tile<FMA, 3, T_QUAD>(d, tile);
-    return;
-  case K_RESTRICT_VC: restrict_vc_tile(d, tile); return;
-  case K_RESTRICT_CC: restrict_cc_tile<FMA>(d, tile); return;
-  case K_PROLONG_VC:
-    if (HIGH) {
-      switch (d.order) {
-      case 7: prolong_ntl<VC<7>, FMA>(d, tile, sm); return;
-      case 9: prolong_ntl<VC<9>, FMA>(d, tile, sm); return;
-      case 11: prolong_ntl<VC<11>, FMA>(d, tile, sm); return;
-      }
-    } else {
-      switch (d.order) {
-      case 1: prolong_ntl<VC<1>, FMA>(d, tile, sm); return;
-      case 3: prolong_ntl<VC<3>, FMA>(d, tile, sm); return;
-      case 5: prolong_ntl<VC<5>, FMA>(d, tile, sm); return;
-      }
-    }
-    break;
-  case K_PROLONG_CC:
-    if (!HIGH) {
-      switch (d.order) {
-      case 0: prolong_ntl<CC<0>, FMA>(d, tile, sm); return;
-      case 1: prolong_ntl<CC<1>, FMA>(d, tile, sm); return;
-      case 2: prolong_ntl<CC<2>, FMA>(d, tile, sm); return;
-      case 3: prolong_ntl<CC<3>, FMA>(d, tile, sm); return;
-      case 4: prolong_ntl<CC<4>, FMA>(d, tile, sm); return;
-      case 5: prolong_ntl<CC<5>, FMA>(d, tile, sm); return;
-      }
-    }
-    break;
-  case K_PROLONG_ENO:
-    if (!HIGH) { prolong_ntl<ENO, FMA>(d, tile, sm); return; }
-    break;
-  }
-  if (threadIdx.x == 0) report(status, CGX_EDEVICE);
-}
-
-template <int FMA, bool HIGH>
-__global__ void __launch_bounds__(NTHREADS, 2)
-    k_pair(const __grid_constant__ Desc d, int *status) {
-  extern __shared__ double sm[];
-  run_tile<FMA, HIGH>(d, blockIdx.x, sm, status);
-}
-
-// Persistent form: each CTA repeatedly claims the next tile index from
-// *counter; prefix[i] is the first global tile of descriptor i.
-template <int FMA>
-__global__ void __launch_bounds__(NTHREADS, 2)
-    k_batch(const Desc *__restrict__ descs, const long long *__restrict__ prefix, int ndesc,
-            long long ntiles, unsigned long long *counter, int *status) {
-  extern __shared__ double sm[];
-  __shared__ long long s_tile;
-  __shared__ int s_desc;
-  for (;;) {
-    if (threadIdx.x == 0) {
-      long long t = (long long)atomicAdd(counter, 1ULL);
-      int lo = 0, hi = ndesc - 1;
-      if (t < ntiles) {
-        while (lo < hi) { // last descriptor with prefix <= t
-          int mid = (lo + hi + 1) >> 1;
-          if (prefix[mid] <= t) lo = mid;
-          else hi = mid - 1;
-        }
-      }
-      s_tile = t;
-      s_desc = lo;
-    }
-    __syncthreads();
-    const long long t = s_tile;
-    const int di = s_desc;
-    __syncthreads(); // everyone has read s_tile before thread 0 rewrites it
-    if (t >= ntiles) break;
-    run_tile<FMA, false>(descs[di], (int)(t - prefix[di]), sm, status);
-  }
-}
-
-} // namespace
 
 // ============================================================== host side
 namespace {
 
 thread_local std::string g_err;
 int g_fp_mode = CGX_FP_EXACT;
-bool g_attr_done[2][2] = {{false, false}, {false, false}};
-bool g_batch_attr_done[2] = {false, false};
 
 int fail(int code, const char *fmt, ...) {
   char buf[512];
@@ -185,11 +68,45 @@ struct Box {
   }
 };
 
-int kind_tiles(int kind, const int *n, int *tiles) {
-  bool prol = kind == K_PROLONG_VC || kind == K_PROLONG_CC || kind == K_PROLONG_ENO;
-  const int t[3] = {prol ? PTX : CTX, prol ? PTY : CTY, prol ? PTZ : CTZ};
+// ceil(2^64 / n) for the device's multiply-high division; 0 encodes n = 1
+unsigned long long reciprocal(int n) {
+  if (n <= 1) return 0;
+  const unsigned __int128 one = (unsigned __int128)1 << 64;
+  return (unsigned long long)((one + (unsigned)n - 1) / (unsigned)n);
+}
+
+// Tiles of a descriptor.  Prolongation: ptx fine x (<= PTXMAX) by
+// 2*ptyc-1 fine y by PTZ fine z, the widths balanced over the region so that
+// thin regions get narrow, tall tiles.  Copy and restriction: crows rows
+// (j,k) of about CTARGET points.
+int kind_tiles(Desc &d) {
+  const int kind = d.kind;
+  const bool prol = kind == K_PROLONG_VC || kind == K_PROLONG_CC || kind == K_PROLONG_ENO;
   long long tot = 1;
-  for (int d = 0; d < 3; ++d) { tiles[d] = (n[d] + t[d] - 1) / t[d]; tot *= tiles[d]; }
+  if (prol) {
+    const int ntx = (d.n[0] + PTXMAX - 1) / PTXMAX;
+    const int ptx = (d.n[0] + ntx - 1) / ntx;
+    int ptyc = std::min(PTYCMAX, NTHREADS / ptx);
+    const int nty = (d.n[1] + 2 * ptyc - 2) / (2 * ptyc - 1);
+    const int pty = (d.n[1] + nty - 1) / nty;
+    ptyc = std::min(ptyc, (pty + 2) / 2);
+    d.ptx = (unsigned char)ptx;
+    d.ptyc = (unsigned char)ptyc;
+    d.tiles[0] = (d.n[0] + ptx - 1) / ptx;
+    d.tiles[1] = (d.n[1] + 2 * ptyc - 2) / (2 * ptyc - 1);
+    d.tiles[2] = (d.n[2] + PTZ - 1) / PTZ;
+    for (int k = 0; k < 3; ++k) tot *= d.tiles[k];
+  } else {
+    const long long rows = (long long)d.n[1] * d.n[2];
+    if (rows * d.n[0] >= (1LL << 31)) return -1;
+    const int crows = std::max(1, std::min(65535, CTARGET / d.n[0]));
+    d.crows = (unsigned short)crows;
+    d.tiles[0] = (int)((rows + crows - 1) / crows);
+    d.tiles[1] = d.tiles[2] = 1;
+    tot = d.tiles[0];
+    d.rcp0 = reciprocal(d.n[0]);
+    d.rcp1 = reciprocal(d.n[1]);
+  }
   return tot > 0x7fffffff ? -1 : (int)tot;
 }
 
@@ -541,47 +458,22 @@ int build(int op, int cent, const cgx_array *dst, const cgx_array *srcs, const d
   // read once (copy and restrictions counted per point above)
   const long long src_bytes = b.bytes - 8 * b.points; // one timelevel's reads
   b.bytes = 8 * b.points + (long long)ntl * src_bytes;
-  b.ntiles = kind_tiles(d.kind, d.n, d.tiles);
+  b.ntiles = kind_tiles(d);
   if (b.ntiles <= 0) return fail(CGX_EINVAL, "transfer: region too large");
   *out = b;
   return CGX_OK;
 }
 
-size_t smem_bytes_low() { return sizeof(double) * smem_doubles<5>(); }
-size_t smem_bytes_high() { return sizeof(double) * smem_doubles<11>(); }
-
-template <int FMA, bool HIGH> int ensure_pair_attr() {
-  if (!g_attr_done[FMA][HIGH]) {
-    cudaError_t e = cudaFuncSetAttribute(k_pair<FMA, HIGH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(HIGH ? smem_bytes_high() : smem_bytes_low()));
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
-    g_attr_done[FMA][HIGH] = true;
-  }
-  return CGX_OK;
-}
-
 int launch_pair(const Desc &d, int ntiles, int fp, int *status, cudaStream_t s) {
   const bool high = d.kind == K_PROLONG_VC && d.order >= 7;
-  int rc;
-  if (fp == CGX_FP_FMA) {
-    if (high) {
-      if ((rc = ensure_pair_attr<1, true>())) return rc;
-      k_pair<1, true><<<ntiles, NTHREADS, smem_bytes_high(), s>>>(d, status);
-    } else {
-      if ((rc = ensure_pair_attr<1, false>())) return rc;
-      k_pair<1, false><<<ntiles, NTHREADS, smem_bytes_low(), s>>>(d, status);
-    }
-  } else {
-    if (high) {
-      if ((rc = ensure_pair_attr<0, true>())) return rc;
-      k_pair<0, true><<<ntiles, NTHREADS, smem_bytes_high(), s>>>(d, status);
-    } else {
-      if ((rc = ensure_pair_attr<0, false>())) return rc;
-      k_pair<0, false><<<ntiles, NTHREADS, smem_bytes_low(), s>>>(d, status);
-    }
-  }
-  cudaError_t e = cudaGetLastError();
-  return e == cudaSuccess ? CGX_OK : cuda_fail(e, "kernel launch");
+  if (high) return klaunch_pair_hi(fp, d, ntiles, status, s);
+  return fp == CGX_FP_FMA ? klaunch_pair_f1(d, ntiles, status, s) : klaunch_pair_f0(d, ntiles, status, s);
+}
+
+int launch_map(int fp, const Desc *d, const int2 *tmap, long long ntiles, unsigned long long *counter,
+               int *status, cudaStream_t s) {
+  return fp == CGX_FP_FMA ? klaunch_map_f1(d, tmap, ntiles, counter, status, s)
+                          : klaunch_map_f0(d, tmap, ntiles, counter, status, s);
 }
 
 } // namespace
@@ -595,6 +487,8 @@ struct cgx_batch {
   Desc *d_descs = nullptr;
   long long *d_prefix = nullptr;
   size_t d_cap = 0;
+  int2 *d_tmap = nullptr; // (descriptor, local tile) of every queued tile
+  size_t tmap_cap = 0;
   int n_uploaded = 0;     // descriptors in the persistent kernel's queue
   long long tiles_uploaded = 0;
   std::vector<int> high_idx; // descriptors launched per box
@@ -669,6 +563,7 @@ int cgx_batch_destroy(cgx_batch *b) {
   if (!b) return CGX_OK;
   cudaFree(b->d_descs);
   cudaFree(b->d_prefix);
+  cudaFree(b->d_tmap);
   cudaFree(b->d_counter);
   cudaFree(b->d_status);
   delete b;
@@ -748,10 +643,23 @@ int cgx_batch_upload(cgx_batch *b, void *stream) {
   b->n_uploaded = (int)n;
   b->tiles_uploaded = acc;
   b->fp_mode = g_fp_mode;
+  if ((size_t)acc > b->tmap_cap) {
+    cudaFree(b->d_tmap);
+    b->d_tmap = nullptr;
+    size_t cap = std::max<size_t>((size_t)acc, 1024);
+    cudaError_t e = cudaMalloc(&b->d_tmap, cap * sizeof(int2));
+    if (e != cudaSuccess) { b->tmap_cap = 0; return cuda_fail(e, "cudaMalloc"); }
+    b->tmap_cap = cap;
+  }
+  std::vector<int2> hm((size_t)acc);
+  for (size_t i = 0; i < n; ++i)
+    for (int k = 0; k < b->ntiles[order[i]]; ++k) hm[(size_t)hp[i] + k] = make_int2((int)i, k);
   if (n) {
     cudaError_t e = cudaMemcpyAsync(b->d_descs, hd.data(), n * sizeof(Desc), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(b->d_prefix, hp.data(), n * sizeof(long long), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(b->d_tmap, hm.data(), hm.size() * sizeof(int2), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s); // host vectors are temporaries
     if (e != cudaSuccess) return cuda_fail(e, "descriptor upload");
   }
@@ -764,27 +672,10 @@ int cgx_batch_launch(cgx_batch *b, void *stream) {
   if (b->n_uploaded > 0) {
     cudaError_t e = cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
-    int dev = 0, nsm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const int fp = b->fp_mode;
-    const size_t smem = smem_bytes_low();
-    if (!g_batch_attr_done[fp]) {
-      e = cudaFuncSetAttribute(fp ? k_batch<1> : k_batch<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem);
-      if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
-      g_batch_attr_done[fp] = true;
-    }
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fp ? k_batch<1> : k_batch<0>, NTHREADS, smem);
-    if (e != cudaSuccess || per_sm < 1) per_sm = 1;
-    long long grid = std::min<long long>((long long)nsm * per_sm, b->tiles_uploaded);
-    if (fp) k_batch<1><<<(int)grid, NTHREADS, smem, s>>>(b->d_descs, b->d_prefix, b->n_uploaded,
-                                                          b->tiles_uploaded, b->d_counter, b->d_status);
-    else k_batch<0><<<(int)grid, NTHREADS, smem, s>>>(b->d_descs, b->d_prefix, b->n_uploaded,
-                                                       b->tiles_uploaded, b->d_counter, b->d_status);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(e, "k_batch launch");
+    int rc = launch_map(b->fp_mode, b->d_descs, b->d_tmap, b->tiles_uploaded, b->d_counter,
+                        b->d_status, s);
+    if (rc) return rc;
+
   }
   for (int i : b->high_idx) {
     int rc = launch_pair(b->descs[i], b->ntiles[i], b->fp_mode, b->d_status, s);
@@ -962,23 +853,64 @@ extern "C" int cgx_transfer_pairs_noalloc(const cgx_pair *pairs, int npairs, voi
   // the work counter and the status word start at zero on every call
   cudaError_t e = cudaMemsetAsync(base + kNoAllocCounterOff, 0, 256, s);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
-  int dev = 0, nsm = 0, per_sm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const int fp = g_fp_mode;
-  const size_t smem = smem_bytes_low();
-  if (!g_batch_attr_done[fp]) {
-    e = cudaFuncSetAttribute(fp ? k_batch<1> : k_batch<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
-    g_batch_attr_done[fp] = true;
-  }
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fp ? k_batch<1> : k_batch<0>, NTHREADS,
-                                                    smem);
-  if (e != cudaSuccess || per_sm < 1) per_sm = 1;
-  const long long grid = std::min<long long>((long long)nsm * per_sm, tiles);
-  if (fp) k_batch<1><<<(int)grid, NTHREADS, smem, s>>>(d_descs, d_prefix, npairs, tiles, d_counter, d_status);
-  else k_batch<0><<<(int)grid, NTHREADS, smem, s>>>(d_descs, d_prefix, npairs, tiles, d_counter, d_status);
-  e = cudaGetLastError();
-  return e == cudaSuccess ? CGX_OK : cuda_fail(e, "k_batch launch");
+  return g_fp_mode == CGX_FP_FMA
+             ? klaunch_search_f1(d_descs, d_prefix, npairs, tiles, d_counter, d_status, s)
+             : klaunch_search_f0(d_descs, d_prefix, npairs, tiles, d_counter, d_status, s);
 }
+
+// ============================================================== internal API
+namespace cgx {
+
+int host_build(int op, int cent, const cgx_array *dst, const cgx_array *srcs, const double *times,
+               int nsrc, const int *dstbox, const int *srcbox, const int *slab, double time,
+               int order_space, int order_time, BuiltPair *out) {
+  Built b;
+  int rc = build(op, cent, dst, srcs, times, nsrc, dstbox, srcbox, slab, time, order_space,
+                 order_time, &b);
+  if (rc) return rc;
+  out->d = b.d;
+  out->bytes = b.bytes;
+  out->points = b.points;
+  out->ntiles = b.ntiles;
+  return CGX_OK;
+}
+
+int batch_pairs(const cgx_batch *b, const Desc **descs, const int **ntiles, const long long **points,
+                int *n) {
+  if (!b) return fail(CGX_EINVAL, "null batch");
+  for (size_t i = 0; i < b->high.size(); ++i)
+    if (b->high[i]) return fail(CGX_EUNSUPPORTED, "vertex-centred orders 7-11 cannot be served");
+  *descs = b->descs.data();
+  *ntiles = b->ntiles.data();
+  *points = b->points.data();
+  *n = (int)b->descs.size();
+  return CGX_OK;
+}
+
+int launch_tile_map(const Desc *d_descs, const int2 *d_tmap, long long ntiles,
+                    unsigned long long *d_counter, int *d_status, int fp, cudaStream_t s) {
+  if (ntiles <= 0) return CGX_OK;
+  cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+  return launch_map(fp, d_descs, d_tmap, ntiles, d_counter, d_status, s);
+}
+
+int launch_one_pair(const Desc &d, int ntiles, int fp, int *status, cudaStream_t s) {
+  return launch_pair(d, ntiles, fp, status, s);
+}
+
+int current_fp_mode() { return g_fp_mode; }
+
+int set_error(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+int cuda_error(cudaError_t e, const char *what) { return cuda_fail(e, what); }
+
+} // namespace cgx

@@ -13,6 +13,8 @@
 // to the reference built without contraction.
 #pragma once
 #include <cstdint>
+#include <type_traits>
+#include <utility>
 
 namespace cgx {
 
@@ -30,11 +32,17 @@ enum TKind : int { T_NONE = 0, T_LIN = 1, T_QUAD = 2, T_ENO = 3 };
 
 // Tile geometry.
 constexpr int NTHREADS = 256;
-// prolongation: 32 fine x (one per lane) by 14 fine y (8 coarse rows, one
-// per warp) by a z chunk marched plane by plane
-constexpr int PTX = 32, PTY = 14, PTZ = 32;
-// copy / restriction: 32 x by 8 y by 8 z destination points
-constexpr int CTX = 32, CTY = 8, CTZ = 8;
+constexpr int NWARPS = NTHREADS / 32;
+// prolongation: a tile is ptx fine x (at most PTXMAX, so at most 16 coarse
+// bases) by 2*ptyc-1 fine y (at most ptyc coarse rows) by a PTZ chunk of fine
+// z that the CTA marches plane by plane.  ptx and ptyc are chosen per
+// descriptor (thin regions get narrow, tall tiles); ptx*ptyc <= NTHREADS,
+// one thread per (fine x, coarse y row) column.
+constexpr int PTXMAX = 30, PTYCMAX = 16, PTZ = 64;
+// copy / restriction: a tile is crows consecutive rows (j,k) of the region,
+// about CTARGET points; CU rows (or packed row groups) per warp are in
+// flight at a time
+constexpr int CTARGET = 16384, CU = 4;
 
 struct Desc {
   int kind, order, ntl, tkind;
@@ -43,13 +51,24 @@ struct Desc {
   int doff[3];  // destination index of the region start
   int sext[3];  // logical extent of the source arrays (load clamp)
   int tiles[3]; // tile grid over the region
-  int pad_;
+  unsigned char ptx, ptyc; // prolongation tile shape (fine x, coarse y rows)
+  unsigned short crows;    // copy/restriction tile: region rows (j,k) per tile
   long long ssy, ssz; // source strides (elements) in y and z
   long long dsy, dsz; // destination strides
+  unsigned long long rcp0, rcp1; // ceil(2^64 / n[0]), ceil(2^64 / n[1]); 0 for 1
   const double *src[3];
   double *dst;
   double w[8]; // time weights (layout of the oracle's cgxo_time_weights)
 };
+
+// compile-time loop: f(std::integral_constant<int, 0>()) ... f(<N-1>)
+template <class Fn, int... I>
+__device__ __forceinline__ void static_for_impl(Fn &&f, std::integer_sequence<int, I...>) {
+  (f(std::integral_constant<int, I>()), ...);
+}
+template <int N, class Fn> __device__ __forceinline__ void static_for(Fn &&f) {
+  static_for_impl(f, std::make_integer_sequence<int, N>());
+}
 
 // ---------------------------------------------------------------- arithmetic
 template <int FMA> __device__ __forceinline__ double madd(double a, double b, double c) {
@@ -217,60 +236,124 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 // restrict_3d_rf2 (restrict_3d_rf2.cc:102-108) and restrict_3d_cc_rf2
 // (restrict_3d_cc_rf2.cc:246-262).  soff is the source index of the region
 // start; the restrictions step by 2 in the source.
-template <int FMA, int NTL, int TK>
-__device__ void copy_tile(const Desc &d, int tile) {
-  int tx = tile % d.tiles[0], r = tile / d.tiles[0];
-  int ty = r % d.tiles[1], tz = r / d.tiles[1];
-  int i = tx * CTX + (threadIdx.x & 31);
-  int j = ty * CTY + (threadIdx.x >> 5);
-  if (i >= d.n[0] || j >= d.n[1]) return;
-  int k0 = tz * CTZ, k1 = min(k0 + CTZ, d.n[2]);
-  for (int k = k0; k < k1; ++k) {
-    long long si = (d.soff[0] + i) + (d.soff[1] + j) * d.ssy + (d.soff[2] + k) * d.ssz;
-    double v[NTL];
+//
+// These are pure streaming operations on regions of any shape -- ghost
+// zones are 3 points thin in one direction -- so a tile is a run of region
+// rows, streamed with lanes along x and short rows packed several to a
+// warp access; a row index is split into (j,k) by multiply-high with a
+// precomputed reciprocal.
+
+// floor(p / n) for p, n < 2^32 given M = ceil(2^64 / n) (M = 0 for n = 1)
+__device__ __forceinline__ unsigned div_rcp(unsigned p, unsigned long long M) {
+  return M ? (unsigned)__umul64hi((unsigned long long)p, M) : p;
+}
+
+// Row-streaming over a tile of the region: every (row, x segment) item is
+// one warp access of up to 32 consecutive x.  Rows shorter than 32 are
+// packed 32/n0 to a warp access.  body_load(item-slot, j, k, i) issues the
+// loads of one point, body_store(item-slot, j, k, i) its store; CU items per
+// warp are loaded before any is stored.
+template <class D, class LoadF, class StoreF>
+__device__ __forceinline__ void stream_rows(D &d, int tile, LoadF &&body_load, StoreF &&body_store) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int n0 = d.n[0], n1 = d.n[1];
+  const unsigned nrows = (unsigned)n1 * d.n[2];
+  const unsigned r0 = (unsigned)tile * d.crows;
+  const unsigned r1 = min(nrows, r0 + d.crows);
+  // segment geometry
+  const bool packed = n0 < 32;
+  const int per = packed ? 32 / n0 : 1;             // rows per item
+  const int nseg = packed ? 1 : (n0 + 31) >> 5;     // items per row
+  const int sub = packed ? lane / n0 : 0;
+  const int li = packed ? lane - sub * n0 : lane;   // x within the segment
+  const unsigned nitems = packed ? (r1 - r0 + per - 1) / per : (r1 - r0) * nseg;
+  for (unsigned it0 = warp; it0 < nitems; it0 += NWARPS * CU) {
+    int jj[CU], kk[CU], ii[CU];
 #pragma unroll
-    for (int t = 0; t < NTL; ++t) v[t] = __ldg(d.src[t] + si);
-    d.dst[(d.doff[0] + i) + (d.doff[1] + j) * d.dsy + (d.doff[2] + k) * d.dsz] =
-        tcombine<FMA, TK, NTL>(d.w, v);
+    for (int u = 0; u < CU; ++u) {
+      const unsigned it = it0 + u * NWARPS;
+      ii[u] = -1;
+      if (it < nitems) {
+        unsigned row;
+        int i;
+        if (packed) {
+          row = r0 + it * per + sub;
+          i = li;
+          if (sub >= per || row >= r1) continue;
+        } else {
+          const unsigned rseg = it / nseg;
+          row = r0 + rseg;
+          i = (int)(it - rseg * nseg) * 32 + li;
+          if (i >= n0) continue;
+        }
+        const unsigned k = div_rcp(row, d.rcp1);
+        jj[u] = (int)(row - k * (unsigned)n1);
+        kk[u] = (int)k;
+        ii[u] = i;
+        body_load(u, jj[u], kk[u], i);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < CU; ++u)
+      if (ii[u] >= 0) body_store(u, jj[u], kk[u], ii[u]);
   }
 }
 
-__device__ void restrict_vc_tile(const Desc &d, int tile) {
-  int tx = tile % d.tiles[0], r = tile / d.tiles[0];
-  int ty = r % d.tiles[1], tz = r / d.tiles[1];
-  int i = tx * CTX + (threadIdx.x & 31);
-  int j = ty * CTY + (threadIdx.x >> 5);
-  if (i >= d.n[0] || j >= d.n[1]) return;
-  int k0 = tz * CTZ, k1 = min(k0 + CTZ, d.n[2]);
-  const double *s = d.src[0];
-  for (int k = k0; k < k1; ++k)
-    d.dst[(d.doff[0] + i) + (d.doff[1] + j) * d.dsy + (d.doff[2] + k) * d.dsz] =
-        __ldg(s + (d.soff[0] + 2 * i) + (d.soff[1] + 2 * j) * d.ssy + (d.soff[2] + 2 * k) * d.ssz);
+template <int FMA, int NTL, int TK, class D>
+__device__ void copy_tile(D &d, int tile) {
+  double v[CU][NTL];
+  stream_rows(
+      d, tile,
+      [&](int u, int j, int k, int i) {
+        const long long si = (d.soff[0] + i) + (d.soff[1] + j) * d.ssy + (d.soff[2] + k) * d.ssz;
+#pragma unroll
+        for (int t = 0; t < NTL; ++t) v[u][t] = __ldg(d.src[t] + si);
+      },
+      [&](int u, int j, int k, int i) {
+        d.dst[(d.doff[0] + i) + (d.doff[1] + j) * d.dsy + (d.doff[2] + k) * d.dsz] =
+            tcombine<FMA, TK, NTL>(d.w, v[u]);
+      });
 }
 
-template <int FMA>
-__device__ void restrict_cc_tile(const Desc &d, int tile) {
-  int tx = tile % d.tiles[0], r = tile / d.tiles[0];
-  int ty = r % d.tiles[1], tz = r / d.tiles[1];
-  int i = tx * CTX + (threadIdx.x & 31);
-  int j = ty * CTY + (threadIdx.x >> 5);
-  if (i >= d.n[0] || j >= d.n[1]) return;
-  int k0 = tz * CTZ, k1 = min(k0 + CTZ, d.n[2]);
+template <class D>
+__device__ void restrict_vc_tile(D &d, int tile) {
+  double v[CU];
   const double *s = d.src[0];
+  stream_rows(
+      d, tile,
+      [&](int u, int j, int k, int i) {
+        v[u] = __ldg(s + (d.soff[0] + 2 * i) + (d.soff[1] + 2 * j) * d.ssy + (d.soff[2] + 2 * k) * d.ssz);
+      },
+      [&](int u, int j, int k, int i) {
+        d.dst[(d.doff[0] + i) + (d.doff[1] + j) * d.dsy + (d.doff[2] + k) * d.dsz] = v[u];
+      });
+}
+
+template <int FMA, class D>
+__device__ void restrict_cc_tile(D &d, int tile) {
+  double v[CU];
   const double w = 0.125; // f1*f1*f1 with f1 = f2 = 1/2
-  for (int k = k0; k < k1; ++k) {
-    const double *p = s + (d.soff[0] + 2 * i) + (d.soff[1] + 2 * j) * d.ssy + (d.soff[2] + 2 * k) * d.ssz;
-    // order of restrict_3d_cc_rf2.cc:253-260
-    double res = mul(w, __ldg(p));
-    res = madd<FMA>(w, __ldg(p + 1), res);
-    res = madd<FMA>(w, __ldg(p + d.ssy), res);
-    res = madd<FMA>(w, __ldg(p + 1 + d.ssy), res);
-    res = madd<FMA>(w, __ldg(p + d.ssz), res);
-    res = madd<FMA>(w, __ldg(p + 1 + d.ssz), res);
-    res = madd<FMA>(w, __ldg(p + d.ssy + d.ssz), res);
-    res = madd<FMA>(w, __ldg(p + 1 + d.ssy + d.ssz), res);
-    d.dst[(d.doff[0] + i) + (d.doff[1] + j) * d.dsy + (d.doff[2] + k) * d.dsz] = res;
-  }
+  stream_rows(
+      d, tile,
+      [&](int u, int j, int k, int i) {
+        const double *q = d.src[0] + (d.soff[0] + 2 * i) + (d.soff[1] + 2 * j) * d.ssy +
+                          (d.soff[2] + 2 * k) * d.ssz;
+        const double a0 = __ldg(q), a1 = __ldg(q + 1), a2 = __ldg(q + d.ssy), a3 = __ldg(q + 1 + d.ssy);
+        const double a4 = __ldg(q + d.ssz), a5 = __ldg(q + 1 + d.ssz);
+        const double a6 = __ldg(q + d.ssy + d.ssz), a7 = __ldg(q + 1 + d.ssy + d.ssz);
+        // order of restrict_3d_cc_rf2.cc:253-260
+        double res = mul(w, a0);
+        res = madd<FMA>(w, a1, res);
+        res = madd<FMA>(w, a2, res);
+        res = madd<FMA>(w, a3, res);
+        res = madd<FMA>(w, a4, res);
+        res = madd<FMA>(w, a5, res);
+        res = madd<FMA>(w, a6, res);
+        v[u] = madd<FMA>(w, a7, res);
+      },
+      [&](int u, int j, int k, int i) {
+        d.dst[(d.doff[0] + i) + (d.doff[1] + j) * d.dsy + (d.doff[2] + k) * d.dsz] = v[u];
+      });
 }
 
 // ---------------------------------------------------------------- prolongation
@@ -279,33 +362,34 @@ __device__ void restrict_cc_tile(const Desc &d, int tile) {
 //   x-pass rows    NTL x CY x PTX
 template <class F> struct PGeom {
   static constexpr int W = F::HI - F::LO;         // window width - 1
-  static constexpr int CX = PTX / 2 + 1 + W;      // coarse x per plane
+  static constexpr int CX = 16 + W;               // coarse x per plane (16 bases)
   static constexpr int CXP = CX + (CX % 2 == 0);  // odd row pitch: fewer bank conflicts
-  static constexpr int CY = PTY / 2 + 1 + W;      // coarse y per plane
+  static constexpr int CY = PTYCMAX + W;          // coarse y per plane
   static constexpr int Q = W + 1;                 // z window (register queue)
   static constexpr int PD = 2;                    // prefetch distance (planes)
-  static constexpr int NB = PD + 1;               // ring buffer depth
-  static constexpr int XR = PTX + 1;              // x-pass row pitch
+  static constexpr int NB = PD + 2;               // staging ring slots
+  static constexpr int XR = 34;                   // x-pass row pitch (2 x 16 + 2)
 };
 template <class F, int NTL> struct PSmem {
   using G = PGeom<F>;
   static constexpr int plane = G::CY * G::CXP;
-  static constexpr int coarse = G::NB * NTL * plane;
-  static constexpr int xrows = NTL * G::CY * G::XR;
-  static constexpr int total = coarse + xrows; // doubles
+  static constexpr int coarse = (G::NB * NTL * plane + 1) / 2 * 2; // x-pass rows 16-B aligned
+  static constexpr int xbuf = NTL * G::CY * G::XR; // one plane of x-pass rows
+  static constexpr int total = coarse + 2 * xbuf;   // doubles
 };
 
-template <class F, int FMA, int NTL, int TK>
-__device__ void prolong_tile(const Desc &d, int tile, double *sm) {
+template <class F, int FMA, int NTL, int TK, class D>
+__device__ void prolong_tile(D &d, int tile, double *sm) {
   using G = PGeom<F>;
   using S = PSmem<F, NTL>;
-  constexpr int LO = F::LO, HI = F::HI, Q = G::Q;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int LO = F::LO, HI = F::HI, Q = G::Q, W = G::W;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ptx = d.ptx, ptyc = d.ptyc, pty = 2 * ptyc - 1;
 
-  int tx = tile % d.tiles[0], rr = tile / d.tiles[0];
-  int ty = rr % d.tiles[1], tz = rr / d.tiles[1];
-  const int fx0 = tx * PTX, fy0 = ty * PTY, fz0 = tz * PTZ;
-  const int nfx = min(PTX, d.n[0] - fx0), nfy = min(PTY, d.n[1] - fy0), nfz = min(PTZ, d.n[2] - fz0);
+  const int tx = tile % d.tiles[0], rr = tile / d.tiles[0];
+  const int ty = rr % d.tiles[1], tz = rr / d.tiles[1];
+  const int fx0 = tx * ptx, fy0 = ty * pty, fz0 = tz * PTZ;
+  const int nfx = min(ptx, d.n[0] - fx0), nfy = min(pty, d.n[1] - fy0), nfz = min(PTZ, d.n[2] - fz0);
   // source positions (fine units) of the tile's first points
   const int sx0 = d.soff[0] + fx0, sy0 = d.soff[1] + fy0, sz0 = d.soff[2] + fz0;
   // coarse index ranges held in shared memory
@@ -313,35 +397,69 @@ __device__ void prolong_tile(const Desc &d, int tile, double *sm) {
   const int cy0 = (sy0 >> 1) + LO, cy1 = ((sy0 + nfy - 1) >> 1) + HI;
   const int cz0 = (sz0 >> 1) + LO, cz1 = ((sz0 + nfz - 1) >> 1) + HI;
   const int ncx = cx1 - cx0 + 1, ncy = cy1 - cy0 + 1;
+  const int nrows = NTL * ncy; // staged rows per plane: (timelevel, coarse y)
+  const int c_first = sx0 >> 1, c_last = (sx0 + nfx - 1) >> 1;
+  const int xoff = sx0 - 2 * c_first; // fine x of the tile's first point in x-pass rows
 
   double *coarse = sm;
-  double *xrow = sm + S::coarse;
+  double *xrows = sm + S::coarse;
 
-  // --- stage one coarse plane of every timelevel (clamped to the array)
-  auto stage = [&](int cz, int buf) {
-    const int per = ncx * ncy;
+  // --- staging: warp w copies rows w, w+8, ...; lane = coarse x (< 32)
+  const int gx = cx0 + lane;
+  const bool xin = lane < ncx && gx >= 0 && gx < d.sext[0];
+  auto stage = [&](int cz, int slot) {
     const bool zin = cz >= 0 && cz < d.sext[2];
-    for (int e = threadIdx.x; e < per * NTL; e += NTHREADS) {
-      int t = e / per, q = e - t * per;
-      int yy = q / ncx, xx = q - yy * ncx;
-      int gx = cx0 + xx, gy = cy0 + yy;
-      double *sp = coarse + ((buf * NTL + t) * G::CY + yy) * G::CXP + xx;
-      if (zin && gx >= 0 && gx < d.sext[0] && gy >= 0 && gy < d.sext[1])
-        cp_async8(sp, d.src[t] + gx + gy * d.ssy + (long long)cz * d.ssz);
-      else
-        *sp = 0.0; // never read by a valid output (host checks the stencils)
+    int t = 0, yy = warp;
+    for (int r = warp; r < nrows; r += NWARPS, yy += NWARPS) {
+      while (yy >= ncy) { yy -= ncy; ++t; }
+      if (lane < ncx) {
+        const int gy = cy0 + yy;
+        double *sp = coarse + ((slot * NTL + t) * G::CY + yy) * G::CXP + lane;
+        if (zin && xin && gy >= 0 && gy < d.sext[1])
+          cp_async8(sp, d.src[t] + gx + gy * d.ssy + (long long)cz * d.ssz);
+        else
+          *sp = 0.0; // never read by a valid output (host checks the stencils)
+      }
     }
   };
 
-  // --- y pass owner: lane <-> fine x, warp <-> coarse y row
-  const int my_fx = lane;                 // tile-relative fine x
-  const int my_cy = (sy0 >> 1) + warp;    // coarse y of this thread
-  // the thread's fine y points: source positions 2*my_cy and 2*my_cy+1
-  const int ys0 = 2 * my_cy, ys1 = 2 * my_cy + 1;
-  const bool v0 = ys0 >= sy0 && ys0 < sy0 + nfy && my_fx < nfx;
-  const bool v1 = ys1 >= sy0 && ys1 < sy0 + nfy && my_fx < nfx;
+  // --- x pass: one coarse base per lane (both its fine points, the copy at
+  // 2c and the interpolant at 2c+1), two rows per warp; x-pass rows are
+  // indexed by fine position minus 2*c_first
+  const int ci = lane & 15, half = lane >> 4;
+  const bool cv = ci <= c_last - c_first;
+  auto xpass = [&](int slot, double *__restrict__ xr) {
+    constexpr int RP = (NTL * G::CY + 1) / 2;      // row pairs, upper bound
+    constexpr int RQ = (RP + NWARPS - 1) / NWARPS; // row pairs per warp
+    const double *__restrict__ cs = coarse;
+#pragma unroll
+    for (int q = 0; q < RQ; ++q) {
+      const int r = 2 * (warp + NWARPS * q) + half;
+      if (r < nrows && cv) {
+        const int t = (r >= ncy) + (NTL > 2 && r >= 2 * ncy);
+        const int yy = r - t * ncy;
+        const double *row = cs + ((slot * NTL + t) * G::CY + yy) * G::CXP + (ci - LO);
+        auto get = [&](int m) { return row[m]; };
+        const double xe = F::template first<FMA>(0, get);
+        const double xo = F::template first<FMA>(1, get);
+        *reinterpret_cast<double2 *>(xr + (t * G::CY + yy) * G::XR + 2 * ci) = make_double2(xe, xo);
+      }
+    }
+  };
 
-  double yq[NTL][2][Q]; // z window of y-pass results
+  // --- y/z owner: thread = (fine x, coarse y row), both fine y parities
+  const int my_fx = tid % ptx, my_cyr = tid / ptx;
+  const int my_cy = (sy0 >> 1) + my_cyr;
+  const int ys0 = 2 * my_cy, ys1 = ys0 + 1;
+  const bool act = my_cyr < ptyc && my_fx < nfx;
+  const bool v0 = act && ys0 >= sy0 && ys0 < sy0 + nfy;
+  const bool v1 = act && ys1 >= sy0 && ys1 < sy0 + nfy;
+  const int yrow = my_cy - cy0; // index of coarse row my_cy in the plane
+  double *out = d.dst + (d.doff[0] + fx0 + my_fx) + (long long)(d.doff[1] + fy0) * d.dsy +
+                (long long)(d.doff[2] + fz0) * d.dsz;
+
+  // z window: yq[t][h][s] holds the y-pass result of plane p in slot p % Q
+  double yq[NTL][2][Q];
 #pragma unroll
   for (int t = 0; t < NTL; ++t)
 #pragma unroll
@@ -349,80 +467,69 @@ __device__ void prolong_tile(const Desc &d, int tile, double *sm) {
 #pragma unroll
       for (int q = 0; q < Q; ++q) yq[t][h][q] = 0.0;
 
-  // prologue: planes cz0 .. cz0+PD-1
-#pragma unroll
-  for (int p = 0; p < G::PD; ++p) {
-    if (cz0 + p <= cz1) stage(cz0 + p, p % G::NB);
-    cp_async_commit();
-  }
-
-  const int nplanes = cz1 - cz0 + 1;
-  for (int pi = 0; pi < nplanes; ++pi) {
-    const int cz = cz0 + pi;
-    if (cz + G::PD <= cz1) stage(cz + G::PD, (pi + G::PD) % G::NB);
-    cp_async_commit();
-    cp_async_wait<G::PD>();
-    __syncthreads(); // plane cz visible; previous y pass done with xrow
-    const int buf = pi % G::NB;
-
-    // --- x pass: rows (t, yy) of the plane, one fine x per lane-slot
-    {
-      const int items = NTL * ncy * PTX;
-      for (int e = threadIdx.x; e < items; e += NTHREADS) {
-        int fx = e & (PTX - 1), ty_ = e / PTX;
-        int t = ty_ / ncy, yy = ty_ - t * ncy;
-        if (fx < nfx) {
-          int s = sx0 + fx;
-          const double *row = coarse + ((buf * NTL + t) * G::CY + yy) * G::CXP + ((s >> 1) - cx0);
-          xrow[(t * G::CY + yy) * G::XR + fx] =
-              F::template first<FMA>(s & 1, [&](int m) { return row[m]; });
-        }
-      }
-    }
-    __syncthreads();
-
-    // --- y pass into the z window
-    {
-      const int yrow = my_cy - cy0; // index of coarse row my_cy in the plane
+  // y pass of plane p (slot U = p % Q, static) from its x-pass rows, then
+  // the z outputs whose window plane p completes: coarse base cb = cz - HI,
+  // window planes p-W .. p in slots (U+1+k) % Q
+  auto yzpass = [&](auto Ut, int p, const double *__restrict__ xr) {
+    constexpr int U = decltype(Ut)::value;
+    if (v0 || v1) {
 #pragma unroll
       for (int t = 0; t < NTL; ++t) {
-#pragma unroll
-        for (int q = 0; q < Q - 1; ++q) {
-          yq[t][0][q] = yq[t][0][q + 1];
-          yq[t][1][q] = yq[t][1][q + 1];
-        }
-        if (v0 || v1) {
-          const double *col = xrow + (t * G::CY + yrow) * G::XR + my_fx;
-          auto get = [&](int m) { return col[m * G::XR]; };
-          yq[t][0][Q - 1] = v0 ? F::template next<FMA>(0, get) : 0.0;
-          yq[t][1][Q - 1] = v1 ? F::template next<FMA>(1, get) : 0.0;
-        }
+        const double *col = xr + (t * G::CY + yrow) * G::XR + my_fx + xoff;
+        auto get = [&](int m) { return col[m * G::XR]; };
+        yq[t][0][U] = F::template next<FMA>(0, get);
+        yq[t][1][U] = F::template next<FMA>(1, get);
       }
     }
-
-    // --- z pass: the window now holds coarse planes cz-Q+1 .. cz, i.e.
-    // cb+LO .. cb+HI for the coarse base cb = cz - HI
-    const int cb = cz - HI;
+    const int cb = cz0 + p - HI;
 #pragma unroll
     for (int zp = 0; zp < 2; ++zp) {
       const int zs = 2 * cb + zp;
       if (zs < sz0 || zs >= sz0 + nfz) continue;
-      const long long zoff = (long long)(d.doff[2] + fz0 + (zs - sz0)) * d.dsz;
+      double *o = out + (long long)(zs - sz0) * d.dsz;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         if (!(h ? v1 : v0)) continue;
         double v[NTL];
 #pragma unroll
         for (int t = 0; t < NTL; ++t)
-          v[t] = F::template next<FMA>(zp, [&](int m) { return yq[t][h][m - LO]; });
-        const int fy = (h ? ys1 : ys0) - sy0;
-        d.dst[(d.doff[0] + fx0 + my_fx) + (long long)(d.doff[1] + fy0 + fy) * d.dsy + zoff] =
-            tcombine<FMA, TK, NTL>(d.w, v);
+          v[t] = F::template next<FMA>(zp, [&](int m) { return yq[t][h][(U + 1 + (m - LO)) % Q]; });
+        o[(long long)((h ? ys1 : ys0) - sy0) * d.dsy] = tcombine<FMA, TK, NTL>(d.w, v);
       }
     }
+  };
+
+  // Pipeline, one barrier per plane: iteration i stages plane i+PD, runs
+  // the x pass of plane i into x-pass buffer i%2 and the y/z passes of plane
+  // i-1 from buffer (i-1)%2.  The staging ring has PD+2 slots, so the slot
+  // being refilled was last read two iterations ago.  The loop is unrolled
+  // by Q so that every z-window slot index is a compile-time constant.
+  const int nplanes = cz1 - cz0 + 1;
+#pragma unroll
+  for (int p = 0; p < G::PD; ++p) {
+    if (p < nplanes) stage(cz0 + p, p);
+    cp_async_commit();
+  }
+  auto iteration = [&](auto Ut, int i) {
+    // Ut: the static value of (i - 1) % Q
+    if (i + G::PD < nplanes) stage(cz0 + i + G::PD, (i + G::PD) % G::NB);
+    cp_async_commit();
+    cp_async_wait<G::PD>();
+    __syncthreads();
+    if (i < nplanes) xpass(i % G::NB, xrows + (i & 1) * S::xbuf);
+    if (i >= 1) yzpass(Ut, i - 1, xrows + ((i - 1) & 1) * S::xbuf);
+  };
+  iteration(std::integral_constant<int, Q - 1>(), 0); // i = 0: x pass only
+  for (int i0 = 1; i0 <= nplanes; i0 += Q) {
+    static_for<Q>([&](auto Ut) {
+      constexpr int u = decltype(Ut)::value;
+      const int i = i0 + u;
+      if (i <= nplanes) iteration(std::integral_constant<int, u>(), i);
+    });
   }
   cp_async_wait<0>();
   __syncthreads(); // shared memory free for the next tile
+  (void)W;
 }
 
 } // namespace cgx

@@ -1,0 +1,54 @@
+// cgx_internal.h -- pieces of the library shared between its translation
+// units (not part of the C-ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/cgx.h"
+#include "cgx_device.cuh"
+
+namespace cgx {
+
+// One validated box-pair: the device descriptor, its tile count and its
+// algorithmic traffic.
+struct BuiltPair {
+  Desc d;
+  long long bytes;  // algorithmic bytes (reads + writes)
+  long long points; // destination points written
+  int ntiles;
+};
+
+// Validation and descriptor building of cgx_transfer (cgx.cu).
+int host_build(int op, int cent, const cgx_array *dst, const cgx_array *srcs, const double *times,
+               int nsrc, const int *dstbox, const int *srcbox, const int *slab, double time,
+               int order_space, int order_time, BuiltPair *out);
+
+// The host-side descriptors of a batch (cgx.cu).
+int batch_pairs(const cgx_batch *b, const Desc **descs, const int **ntiles, const long long **points,
+                int *n);
+
+// Persistent-kernel launch over a device tile map (cgx.cu); grid sized to
+// the device.
+int launch_tile_map(const Desc *d_descs, const int2 *d_tmap, long long ntiles,
+                    unsigned long long *d_counter, int *d_status, int fp, cudaStream_t s);
+
+// One plain per-box launch (cgx.cu).
+int launch_one_pair(const Desc &d, int ntiles, int fp, int *status, cudaStream_t s);
+
+// kernel launchers (cgx_kern_f0.cu, cgx_kern_f1.cu, cgx_kern_hi.cu)
+int klaunch_pair_f0(const Desc &d, int ntiles, int *status, cudaStream_t s);
+int klaunch_pair_f1(const Desc &d, int ntiles, int *status, cudaStream_t s);
+int klaunch_pair_hi(int fp, const Desc &d, int ntiles, int *status, cudaStream_t s);
+int klaunch_map_f0(const Desc *d, const int2 *tmap, long long ntiles, unsigned long long *counter,
+                   int *status, cudaStream_t s);
+int klaunch_map_f1(const Desc *d, const int2 *tmap, long long ntiles, unsigned long long *counter,
+                   int *status, cudaStream_t s);
+int klaunch_search_f0(const Desc *d, const long long *prefix, int ndesc, long long ntiles,
+                      unsigned long long *counter, int *status, cudaStream_t s);
+int klaunch_search_f1(const Desc *d, const long long *prefix, int ndesc, long long ntiles,
+                      unsigned long long *counter, int *status, cudaStream_t s);
+
+int current_fp_mode();
+int set_error(int code, const char *fmt, ...);
+int cuda_error(cudaError_t e, const char *what);
+
+} // namespace cgx

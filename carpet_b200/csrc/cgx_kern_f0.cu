@@ -1,0 +1,17 @@
+// cgx_kern_f0.cu -- kernels of floating-point mode 0 (0: two roundings per
+// multiply-add, 1: fused), orders 0-5.
+#include "cgx_kern_launch.cuh"
+
+namespace cgx {
+int klaunch_pair_f0(const Desc &d, int ntiles, int *status, cudaStream_t s) {
+  return kern::launch_pair_t<0, false>(d, ntiles, status, s);
+}
+int klaunch_map_f0(const Desc *d, const int2 *tmap, long long ntiles, unsigned long long *counter,
+                  int *status, cudaStream_t s) {
+  return kern::launch_map_t<0>(d, tmap, ntiles, counter, status, s);
+}
+int klaunch_search_f0(const Desc *d, const long long *prefix, int ndesc, long long ntiles,
+                     unsigned long long *counter, int *status, cudaStream_t s) {
+  return kern::launch_search_t<0>(d, prefix, ndesc, ntiles, counter, status, s);
+}
+} // namespace cgx

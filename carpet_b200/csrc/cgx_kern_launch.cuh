@@ -1,0 +1,68 @@
+// cgx_kern_launch.cuh -- host launchers of one floating-point mode's
+// kernels; included once per mode by cgx_kern_f0.cu / cgx_kern_f1.cu.
+#pragma once
+#include "cgx_kernels.cuh"
+
+namespace cgx {
+namespace kern {
+
+template <int FMA, bool HIGH> int launch_pair_t(const Desc &d, int ntiles, int *status, cudaStream_t s) {
+  static bool attr = false;
+  const size_t smem = smem_bytes(HIGH);
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_pair<FMA, HIGH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute");
+    attr = true;
+  }
+  k_pair<FMA, HIGH><<<ntiles, NTHREADS, smem, s>>>(d, status);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? CGX_OK : cuda_error(e, "k_pair launch");
+}
+
+// grid of a persistent kernel: every CTA slot of the device, at most ntiles
+template <class K> int persistent_grid(K kernel, size_t smem, long long ntiles, int *grid) {
+  int dev = 0, nsm = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, NTHREADS, smem);
+  if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+  *grid = (int)std::min<long long>((long long)nsm * per_sm, ntiles);
+  return CGX_OK;
+}
+
+template <int FMA>
+int launch_map_t(const Desc *d_descs, const int2 *d_tmap, long long ntiles, unsigned long long *d_counter,
+                 int *d_status, cudaStream_t s) {
+  static bool attr = false;
+  const size_t smem = smem_bytes(false);
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_batch_map<FMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute");
+    attr = true;
+  }
+  int grid = 0;
+  persistent_grid(k_batch_map<FMA>, smem, ntiles, &grid);
+  k_batch_map<FMA><<<grid, NTHREADS, smem, s>>>(d_descs, d_tmap, ntiles, d_counter, d_status);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? CGX_OK : cuda_error(e, "k_batch_map launch");
+}
+
+template <int FMA>
+int launch_search_t(const Desc *d_descs, const long long *d_prefix, int ndesc, long long ntiles,
+                    unsigned long long *d_counter, int *d_status, cudaStream_t s) {
+  static bool attr = false;
+  const size_t smem = smem_bytes(false);
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_batch<FMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute");
+    attr = true;
+  }
+  int grid = 0;
+  persistent_grid(k_batch<FMA>, smem, ntiles, &grid);
+  k_batch<FMA><<<grid, NTHREADS, smem, s>>>(d_descs, d_prefix, ndesc, ntiles, d_counter, d_status);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? CGX_OK : cuda_error(e, "k_batch launch");
+}
+
+} // namespace kern
+} // namespace cgx

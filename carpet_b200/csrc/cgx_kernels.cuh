@@ -1,0 +1,201 @@
+// cgx_kernels.cuh -- the kernels: tile dispatch and the three launch forms.
+// Included only by the kernel translation units (cgx_kern_*.cu), each of
+// which instantiates and launches one floating-point mode / order range.
+//
+//   k_pair       grid = the tiles of one descriptor (the plain per-box form);
+//   k_batch_map  persistent, one CTA per SM slot, tiles of many descriptors
+//                taken from a device work counter through a tile map;
+//   k_batch      the same, finding each tile's descriptor by binary search
+//                over tile offsets (the bounded-scratch form of the
+//                no-allocation entry point).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/cgx.h"
+#include "cgx_device.cuh"
+#include "cgx_internal.h"
+
+namespace cgx {
+namespace kern {
+
+__device__ __forceinline__ void report(int *status, int code) {
+  if (status) atomicCAS(status, 0, code);
+}
+
+// dynamic shared memory of the largest variant a kernel dispatches
+template <int MAXORDER> constexpr int smem_doubles() {
+  return PSmem<VC<MAXORDER>, 3>::total > PSmem<CC<5>, 3>::total
+             ? PSmem<VC<MAXORDER>, 3>::total
+             : PSmem<CC<5>, 3>::total;
+}
+
+// Every tile routine is its own non-inlined function, so that each variant
+// gets its own register allocation instead of sharing one across the whole
+// dispatch switch.  The descriptor is always in shared memory.
+template <class F, int FMA, int NTL, int TK>
+__device__ __noinline__ void prolong_entry(const Desc &d, int tile, double *sm) {
+  prolong_tile<F, FMA, NTL, TK>(d, tile, sm);
+}
+template <int FMA, int NTL, int TK>
+__device__ __noinline__ void copy_entry(const Desc &d, int tile) {
+  copy_tile<FMA, NTL, TK>(d, tile);
+}
+static __device__ __noinline__ void restrict_vc_entry(const Desc &d, int tile) { restrict_vc_tile(d, tile); }
+template <int FMA> __device__ __noinline__ void restrict_cc_entry(const Desc &d, int tile) {
+  restrict_cc_tile<FMA>(d, tile);
+}
+
+template <class F, int FMA>
+__device__ __forceinline__ void prolong_ntl(const Desc &d, int tile, double *sm) {
+  switch (d.ntl) {
+  case 1: prolong_entry<F, FMA, 1, T_NONE>(d, tile, sm); break;
+  case 2: prolong_entry<F, FMA, 2, T_LIN>(d, tile, sm); break;
+  default:
+    if (d.tkind == T_ENO) prolong_entry<F, FMA, 3, T_ENO>(d, tile, sm);
+    else prolong_entry<F, FMA, 3, T_QUAD>(d, tile, sm);
+  }
+}
+
+// HIGH selects the vertex-centred orders 7/9/11, which live in their own
+// kernel so that their larger register windows do not lower the occupancy
+// of the common orders.
+template <int FMA, bool HIGH>
+__device__ __forceinline__ void run_tile(const Desc &d, int tile, double *sm, int *status) {
+  switch (d.kind) {
+  case K_COPY:
+    if (d.ntl == 1) copy_entry<FMA, 1, T_NONE>(d, tile);
+    else if (d.ntl == 2) copy_entry<FMA, 2, T_LIN>(d, tile);
+    else if (d.tkind == T_ENO) copy_entry<FMA, 3, T_ENO>(d, tile);
+    else copy_entry<FMA, 3, T_QUAD>(d, tile);
+    return;
+  case K_RESTRICT_VC: restrict_vc_entry(d, tile); return;
+  case K_RESTRICT_CC: restrict_cc_entry<FMA>(d, tile); return;
+  case K_PROLONG_VC:
+    if (HIGH) {
+      switch (d.order) {
+      case 7: prolong_ntl<VC<7>, FMA>(d, tile, sm); return;
+      case 9: prolong_ntl<VC<9>, FMA>(d, tile, sm); return;
+      case 11: prolong_ntl<VC<11>, FMA>(d, tile, sm); return;
+      }
+    } else {
+      switch (d.order) {
+      case 1: prolong_ntl<VC<1>, FMA>(d, tile, sm); return;
+      case 3: prolong_ntl<VC<3>, FMA>(d, tile, sm); return;
+      case 5: prolong_ntl<VC<5>, FMA>(d, tile, sm); return;
+      }
+    }
+    break;
+  case K_PROLONG_CC:
+    if (!HIGH) {
+      switch (d.order) {
+      case 0: prolong_ntl<CC<0>, FMA>(d, tile, sm); return;
+      case 1: prolong_ntl<CC<1>, FMA>(d, tile, sm); return;
+      case 2: prolong_ntl<CC<2>, FMA>(d, tile, sm); return;
+      case 3: prolong_ntl<CC<3>, FMA>(d, tile, sm); return;
+      case 4: prolong_ntl<CC<4>, FMA>(d, tile, sm); return;
+      case 5: prolong_ntl<CC<5>, FMA>(d, tile, sm); return;
+      }
+    }
+    break;
+  case K_PROLONG_ENO:
+    if (!HIGH) { prolong_ntl<ENO, FMA>(d, tile, sm); return; }
+    break;
+  }
+  if (threadIdx.x == 0) report(status, CGX_EDEVICE);
+}
+
+template <int FMA, bool HIGH>
+__global__ void __launch_bounds__(NTHREADS, 2)
+    k_pair(const __grid_constant__ Desc d, int *status) {
+  extern __shared__ __align__(16) double sm[];
+  __shared__ __align__(16) Desc s_d;
+  if (threadIdx.x == 0) s_d = d; // field-wise copy out of the parameter space
+  __syncthreads();
+  run_tile<FMA, HIGH>(s_d, blockIdx.x, sm, status);
+}
+
+// Persistent form: each CTA repeatedly claims the next tile index from
+// *counter; prefix[i] is the first global tile of descriptor i.
+template <int FMA>
+__global__ void __launch_bounds__(NTHREADS, 2)
+    k_batch(const Desc *__restrict__ descs, const long long *__restrict__ prefix, int ndesc,
+            long long ntiles, unsigned long long *counter, int *status) {
+  extern __shared__ __align__(16) double sm[];
+  __shared__ long long s_tile;
+  __shared__ int s_desc;
+  // the claimed descriptor, staged in shared memory: tile code reads it like
+  // the kernel-parameter descriptor of k_pair
+  __shared__ __align__(16) Desc s_d;
+  static_assert(sizeof(Desc) % 8 == 0 && sizeof(Desc) / 8 <= NTHREADS, "descriptor staging");
+  for (;;) {
+    if (threadIdx.x == 0) {
+      long long t = (long long)atomicAdd(counter, 1ULL);
+      int lo = 0, hi = ndesc - 1;
+      if (t < ntiles) {
+        while (lo < hi) { // last descriptor with prefix <= t
+          int mid = (lo + hi + 1) >> 1;
+          if (prefix[mid] <= t) lo = mid;
+          else hi = mid - 1;
+        }
+      }
+      s_tile = t;
+      s_desc = lo;
+    }
+    __syncthreads();
+    const long long t = s_tile;
+    const int di = s_desc;
+    if (t >= ntiles) break;
+    if (threadIdx.x < sizeof(Desc) / 8)
+      reinterpret_cast<unsigned long long *>(&s_d)[threadIdx.x] =
+          __ldg(reinterpret_cast<const unsigned long long *>(descs + di) + threadIdx.x);
+    __syncthreads();
+    run_tile<FMA, false>(s_d, (int)(t - prefix[di]), sm, status);
+    __syncthreads(); // s_tile, s_desc and s_d are free for the next claim
+  }
+}
+
+// Persistent form fed by a tile map: tmap[t] = (descriptor, tile within it).
+// Thread 0 claims the next tile when the current one starts, so the
+// claim's round trip overlaps the tile's work; only the map read is exposed.
+template <int FMA>
+__global__ void __launch_bounds__(NTHREADS, 2)
+    k_batch_map(const Desc *__restrict__ descs, const int2 *__restrict__ tmap, long long ntiles,
+                unsigned long long *counter, int *status) {
+  extern __shared__ __align__(16) double sm[];
+  __shared__ long long s_t;
+  __shared__ int2 s_m;
+  __shared__ __align__(16) Desc s_d;
+  if (threadIdx.x == 0) {
+    const long long t = (long long)atomicAdd(counter, 1ULL);
+    s_t = t;
+    s_m = t < ntiles ? tmap[t] : make_int2(0, 0);
+  }
+  __syncthreads();
+  for (;;) {
+    const long long t = s_t;
+    const int2 m = s_m;
+    if (t >= ntiles) break;
+    if (threadIdx.x < sizeof(Desc) / 8)
+      reinterpret_cast<unsigned long long *>(&s_d)[threadIdx.x] =
+          __ldg(reinterpret_cast<const unsigned long long *>(descs + m.x) + threadIdx.x);
+    unsigned long long tn = 0;
+    if (threadIdx.x == 0) tn = atomicAdd(counter, 1ULL);
+    __syncthreads();
+    run_tile<FMA, false>(s_d, m.y, sm, status);
+    __syncthreads(); // everyone is done with s_d, s_t and s_m
+    if (threadIdx.x == 0) {
+      s_t = (long long)tn;
+      s_m = (long long)tn < ntiles ? tmap[tn] : make_int2(0, 0);
+    }
+    __syncthreads();
+  }
+}
+
+
+// dynamic shared memory of the widest variant a kernel dispatches
+inline size_t smem_bytes(bool high) {
+  return sizeof(double) * (high ? smem_doubles<11>() : smem_doubles<5>());
+}
+
+} // namespace kern
+} // namespace cgx

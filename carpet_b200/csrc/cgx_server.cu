@@ -1,0 +1,436 @@
+// cgx_server.cu -- the served form: transfer requests from many independent
+// AMR hierarchies, continuously batched into the persistent kernel.
+//
+// A request names an operation template -- the box-pairs of one transfer
+// (a sync, a boundary prolongation or a restriction of one level of one
+// hierarchy, over all of its grid functions) -- defined once from a
+// cgx_batch.  The worker thread keeps two launch slots.  Whenever a slot is
+// free it takes, in arrival order, the oldest pending request of every
+// hierarchy that has no request on the GPU, concatenates their descriptors
+// into one tile map and launches the persistent kernel on that slot's
+// stream; requests that arrive meanwhile wait only for the next free slot,
+// and the two slots' kernels overlap on the device.  A hierarchy never has
+// two requests in flight, so each hierarchy sees its requests applied one
+// after another in arrival order -- the results are those of running them
+// alone (tests/test_gpu_serving.py).
+//
+// The plain mode serves the same stream through the per-box drop-in: one
+// request at a time, one kernel launch per box-pair.
+//
+// Hierarchies are admitted against an HBM budget (cgx_server_admit /
+// cgx_server_release account the device memory their grid functions use).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "../../include/cgx.h"
+#include "cgx_internal.h"
+
+using namespace cgx;
+
+namespace {
+
+using clk = std::chrono::steady_clock;
+
+struct OpTemplate {
+  int hier;
+  std::vector<Desc> descs;
+  std::vector<int> ntiles;
+  long long tiles = 0, points = 0;
+};
+
+struct Request {
+  int op;
+  double t_arrive = 0, t_launch = 0, t_done = 0; // seconds since the server epoch
+};
+
+struct Slot {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  Desc *d_descs = nullptr, *h_descs = nullptr;
+  int2 *d_tmap = nullptr, *h_tmap = nullptr;
+  unsigned long long *d_counter = nullptr;
+  int *d_status = nullptr;
+  size_t desc_cap = 0, tile_cap = 0;
+  bool busy = false;
+  std::vector<int> reqs;
+};
+
+} // namespace
+
+struct cgx_server {
+  int mode = CGX_SERVE_BATCHED;
+  int fp = CGX_FP_EXACT;
+  long long budget = 0, used = 0;
+  std::vector<OpTemplate> ops;
+  std::vector<Request> reqs; // reserved at creation: never reallocated
+  size_t max_requests = 0;
+  std::vector<char> hier_busy;
+  std::deque<int> pending;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::thread worker;
+  std::atomic<bool> stop{false};
+  std::atomic<long long> completed{0};
+  long long submitted = 0;
+  Slot slots[2];
+  clk::time_point epoch = clk::now();
+  long long launches = 0, batched_requests = 0;
+  int error = CGX_OK;
+
+  double now() const { return std::chrono::duration<double>(clk::now() - epoch).count(); }
+};
+
+namespace {
+
+int slot_init(Slot &s, size_t desc_cap, size_t tile_cap) {
+  cudaError_t e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMalloc(&s.d_descs, desc_cap * sizeof(Desc));
+  if (e == cudaSuccess) e = cudaMallocHost(&s.h_descs, desc_cap * sizeof(Desc));
+  if (e == cudaSuccess) e = cudaMalloc(&s.d_tmap, tile_cap * sizeof(int2));
+  if (e == cudaSuccess) e = cudaMallocHost(&s.h_tmap, tile_cap * sizeof(int2));
+  if (e == cudaSuccess) e = cudaMalloc(&s.d_counter, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&s.d_status, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(s.d_status, 0, sizeof(int));
+  if (e != cudaSuccess) return cuda_error(e, "server slot allocation");
+  s.desc_cap = desc_cap;
+  s.tile_cap = tile_cap;
+  return CGX_OK;
+}
+
+void slot_free(Slot &s) {
+  if (s.stream) cudaStreamSynchronize(s.stream);
+  cudaFree(s.d_descs);
+  cudaFreeHost(s.h_descs);
+  cudaFree(s.d_tmap);
+  cudaFreeHost(s.h_tmap);
+  cudaFree(s.d_counter);
+  cudaFree(s.d_status);
+  if (s.done) cudaEventDestroy(s.done);
+  if (s.stream) cudaStreamDestroy(s.stream);
+  s = Slot();
+}
+
+// Retire a slot whose kernel has finished.
+void retire(cgx_server *sv, Slot &s) {
+  const double t = sv->now();
+  std::lock_guard<std::mutex> g(sv->mu);
+  for (int r : s.reqs) {
+    sv->reqs[r].t_done = t;
+    sv->hier_busy[sv->ops[sv->reqs[r].op].hier] = 0;
+  }
+  sv->completed += (long long)s.reqs.size();
+  s.reqs.clear();
+  s.busy = false;
+  sv->cv.notify_all();
+}
+
+// Batched mode: take the oldest pending request of every idle hierarchy
+// (in arrival order) that fits the slot, and launch them as one kernel.
+bool launch_batch(cgx_server *sv, Slot &s) {
+  std::vector<int> take;
+  size_t ndesc = 0, ntiles = 0;
+  {
+    std::lock_guard<std::mutex> g(sv->mu);
+    std::vector<char> seen(sv->hier_busy.size(), 0);
+    for (auto it = sv->pending.begin(); it != sv->pending.end();) {
+      const OpTemplate &op = sv->ops[sv->reqs[*it].op];
+      if (sv->hier_busy[op.hier] || seen[op.hier]) {
+        seen[op.hier] = 1; // keep this hierarchy's later requests behind it
+        ++it;
+        continue;
+      }
+      seen[op.hier] = 1;
+      if (ndesc + op.descs.size() > s.desc_cap || ntiles + op.tiles > s.tile_cap) {
+        if (take.empty()) { // larger than a slot (define_op rejects these): drop it
+          sv->error = set_error(CGX_EINVAL, "request larger than a server slot");
+          sv->reqs[*it].t_done = -1.0;
+          sv->completed += 1;
+          it = sv->pending.erase(it);
+          continue;
+        }
+        ++it;
+        continue;
+      }
+      take.push_back(*it);
+      ndesc += op.descs.size();
+      ntiles += op.tiles;
+      sv->hier_busy[op.hier] = 1;
+      it = sv->pending.erase(it);
+    }
+  }
+  if (take.empty()) return false;
+  // concatenate descriptors and tile maps in pinned staging
+  size_t di = 0, ti = 0;
+  const double t = sv->now();
+  for (int r : take) {
+    const OpTemplate &op = sv->ops[sv->reqs[r].op];
+    for (size_t k = 0; k < op.descs.size(); ++k) {
+      s.h_descs[di] = op.descs[k];
+      for (int j = 0; j < op.ntiles[k]; ++j) s.h_tmap[ti++] = make_int2((int)di, j);
+      ++di;
+    }
+    sv->reqs[r].t_launch = t;
+  }
+  cudaMemcpyAsync(s.d_descs, s.h_descs, di * sizeof(Desc), cudaMemcpyHostToDevice, s.stream);
+  cudaMemcpyAsync(s.d_tmap, s.h_tmap, ti * sizeof(int2), cudaMemcpyHostToDevice, s.stream);
+  int rc = launch_tile_map(s.d_descs, s.d_tmap, (long long)ti, s.d_counter, s.d_status, sv->fp,
+                           s.stream);
+  if (rc) sv->error = rc;
+  cudaEventRecord(s.done, s.stream);
+  s.reqs = take;
+  s.busy = true;
+  sv->launches++;
+  sv->batched_requests += (long long)take.size();
+  return true;
+}
+
+// Plain mode: one request, one launch per box-pair, in arrival order.
+bool launch_plain(cgx_server *sv, Slot &s) {
+  int r;
+  {
+    std::lock_guard<std::mutex> g(sv->mu);
+    if (sv->pending.empty()) return false;
+    r = sv->pending.front();
+    sv->pending.pop_front();
+  }
+  const OpTemplate &op = sv->ops[sv->reqs[r].op];
+  sv->reqs[r].t_launch = sv->now();
+  for (size_t k = 0; k < op.descs.size(); ++k) {
+    int rc = launch_one_pair(op.descs[k], op.ntiles[k], sv->fp, s.d_status, s.stream);
+    if (rc) sv->error = rc;
+  }
+  cudaEventRecord(s.done, s.stream);
+  s.reqs.assign(1, r);
+  s.busy = true;
+  sv->launches += (long long)op.descs.size();
+  sv->batched_requests += 1;
+  return true;
+}
+
+void worker_loop(cgx_server *sv) {
+  const int nslots = sv->mode == CGX_SERVE_BATCHED ? 2 : 1;
+  for (;;) {
+    bool progress = false;
+    for (int i = 0; i < nslots; ++i) {
+      Slot &s = sv->slots[i];
+      if (s.busy && cudaEventQuery(s.done) == cudaSuccess) {
+        retire(sv, s);
+        progress = true;
+      }
+    }
+    for (int i = 0; i < nslots; ++i) {
+      Slot &s = sv->slots[i];
+      if (!s.busy) {
+        bool l = sv->mode == CGX_SERVE_BATCHED ? launch_batch(sv, s) : launch_plain(sv, s);
+        progress |= l;
+      }
+    }
+    if (progress) continue;
+    bool any_busy = false;
+    for (int i = 0; i < nslots; ++i) any_busy |= sv->slots[i].busy;
+    if (sv->stop.load() && !any_busy) {
+      std::lock_guard<std::mutex> g(sv->mu);
+      if (sv->pending.empty()) return;
+    }
+    if (any_busy) {
+      std::this_thread::yield(); // poll the in-flight slots
+    } else {
+      std::unique_lock<std::mutex> g(sv->mu);
+      sv->cv.wait_for(g, std::chrono::microseconds(200),
+                      [&] { return !sv->pending.empty() || sv->stop.load(); });
+    }
+  }
+}
+
+double percentile(std::vector<double> v, double p) {
+  if (v.empty()) return 0.0;
+  std::sort(v.begin(), v.end());
+  double idx = p * (double)(v.size() - 1);
+  size_t lo = (size_t)idx;
+  size_t hi = std::min(lo + 1, v.size() - 1);
+  double f = idx - (double)lo;
+  return v[lo] * (1 - f) + v[hi] * f;
+}
+
+} // namespace
+
+extern "C" {
+
+int cgx_server_create(cgx_server **out, int mode, int64_t hbm_budget_bytes, int max_pairs,
+                      int64_t max_tiles, int64_t max_requests) {
+  if (!out || max_requests <= 0) return set_error(CGX_EINVAL, "bad server arguments");
+  if (mode != CGX_SERVE_BATCHED && mode != CGX_SERVE_PLAIN)
+    return set_error(CGX_EINVAL, "bad serving mode");
+  if (max_pairs <= 0 || max_tiles <= 0) return set_error(CGX_EINVAL, "bad slot capacity");
+  cgx_server *sv = new cgx_server();
+  sv->mode = mode;
+  sv->budget = hbm_budget_bytes;
+  sv->fp = current_fp_mode();
+  sv->max_requests = (size_t)max_requests;
+  sv->reqs.reserve(sv->max_requests);
+  for (int i = 0; i < 2; ++i) {
+    int rc = slot_init(sv->slots[i], (size_t)max_pairs, (size_t)max_tiles);
+    if (rc) {
+      for (int j = 0; j <= i; ++j) slot_free(sv->slots[j]);
+      delete sv;
+      return rc;
+    }
+  }
+  *out = sv;
+  return CGX_OK;
+}
+
+int cgx_server_destroy(cgx_server *sv) {
+  if (!sv) return CGX_OK;
+  if (sv->worker.joinable()) {
+    sv->stop = true;
+    sv->cv.notify_all();
+    sv->worker.join();
+  }
+  for (int i = 0; i < 2; ++i) slot_free(sv->slots[i]);
+  delete sv;
+  return CGX_OK;
+}
+
+int cgx_server_admit(cgx_server *sv, int64_t bytes) {
+  if (!sv || bytes < 0) return set_error(CGX_EINVAL, "bad admission");
+  std::lock_guard<std::mutex> g(sv->mu);
+  if (sv->used + bytes > sv->budget)
+    return set_error(CGX_ENOMEM, "HBM budget: %lld of %lld bytes in use, %lld more requested",
+                     (long long)sv->used, (long long)sv->budget, (long long)bytes);
+  sv->used += bytes;
+  return CGX_OK;
+}
+
+int cgx_server_release(cgx_server *sv, int64_t bytes) {
+  if (!sv || bytes < 0) return set_error(CGX_EINVAL, "bad release");
+  std::lock_guard<std::mutex> g(sv->mu);
+  sv->used = std::max<long long>(0, sv->used - bytes);
+  return CGX_OK;
+}
+
+int cgx_server_define_op(cgx_server *sv, int hier, const cgx_batch *pairs, int *op_id) {
+  if (!sv || !op_id || hier < 0) return set_error(CGX_EINVAL, "bad operation");
+  if (sv->worker.joinable()) return set_error(CGX_EINVAL, "define operations before starting");
+  const Desc *d;
+  const int *nt;
+  const long long *pts;
+  int n;
+  int rc = batch_pairs(pairs, &d, &nt, &pts, &n);
+  if (rc) return rc;
+  OpTemplate op;
+  op.hier = hier;
+  op.descs.assign(d, d + n);
+  op.ntiles.assign(nt, nt + n);
+  for (int i = 0; i < n; ++i) { op.tiles += nt[i]; op.points += pts[i]; }
+  if (op.descs.size() > sv->slots[0].desc_cap || (size_t)op.tiles > sv->slots[0].tile_cap)
+    return set_error(CGX_EINVAL, "operation larger than a server slot");
+  sv->ops.push_back(std::move(op));
+  if ((int)sv->hier_busy.size() <= hier) sv->hier_busy.resize(hier + 1, 0);
+  *op_id = (int)sv->ops.size() - 1;
+  return CGX_OK;
+}
+
+int cgx_server_start(cgx_server *sv) {
+  if (!sv) return set_error(CGX_EINVAL, "null server");
+  if (sv->worker.joinable()) return CGX_OK;
+  sv->stop = false;
+  sv->fp = current_fp_mode();
+  sv->epoch = clk::now();
+  sv->worker = std::thread(worker_loop, sv);
+  return CGX_OK;
+}
+
+int cgx_server_submit(cgx_server *sv, int op_id, int64_t *request_id) {
+  if (!sv || op_id < 0 || op_id >= (int)sv->ops.size()) return set_error(CGX_EINVAL, "bad request");
+  {
+    std::lock_guard<std::mutex> g(sv->mu);
+    if (sv->reqs.size() >= sv->max_requests)
+      return set_error(CGX_ENOMEM, "request log full (%zu requests)", sv->max_requests);
+    Request r;
+    r.op = op_id;
+    r.t_arrive = sv->now();
+    sv->reqs.push_back(r);
+    sv->pending.push_back((int)sv->reqs.size() - 1);
+    sv->submitted++;
+    if (request_id) *request_id = (int64_t)sv->reqs.size() - 1;
+  }
+  sv->cv.notify_all();
+  return CGX_OK;
+}
+
+int cgx_server_replay(cgx_server *sv, const int *op_ids, const double *arrival_s, int n) {
+  if (!sv || (n > 0 && (!op_ids || !arrival_s))) return set_error(CGX_EINVAL, "bad trace");
+  int rc = cgx_server_start(sv);
+  if (rc) return rc;
+  const double t0 = sv->now();
+  for (int i = 0; i < n; ++i) {
+    const double due = t0 + arrival_s[i];
+    while (sv->now() < due) { /* spin: sub-microsecond arrival accuracy */ }
+    if ((rc = cgx_server_submit(sv, op_ids[i], nullptr))) return rc;
+  }
+  return CGX_OK;
+}
+
+int cgx_server_drain(cgx_server *sv) {
+  if (!sv) return set_error(CGX_EINVAL, "null server");
+  std::unique_lock<std::mutex> g(sv->mu);
+  // bounded: a stream of work that does not finish in 10 minutes is an error
+  if (!sv->cv.wait_for(g, std::chrono::seconds(600),
+                       [&] { return sv->completed.load() >= sv->submitted; }))
+    return set_error(CGX_ECUDA, "server drain timed out");
+  return sv->error;
+}
+
+int cgx_server_stats(cgx_server *sv, cgx_server_report *rep) {
+  if (!sv || !rep) return set_error(CGX_EINVAL, "null argument");
+  std::lock_guard<std::mutex> g(sv->mu);
+  std::vector<double> lat;
+  double first = 1e300, last = 0;
+  long long points = 0, done = 0;
+  for (const Request &r : sv->reqs) {
+    if (r.t_done <= 0) continue;
+    lat.push_back(1e3 * (r.t_done - r.t_arrive));
+    first = std::min(first, r.t_arrive);
+    last = std::max(last, r.t_done);
+    points += sv->ops[r.op].points;
+    ++done;
+  }
+  memset(rep, 0, sizeof *rep);
+  rep->requests = done;
+  rep->launches = sv->launches;
+  rep->p50_ms = percentile(lat, 0.50);
+  rep->p99_ms = percentile(lat, 0.99);
+  rep->mean_ms = lat.empty() ? 0 : [&] { double s = 0; for (double x : lat) s += x; return s / lat.size(); }();
+  rep->makespan_s = done ? last - first : 0;
+  rep->fine_points = points;
+  rep->points_per_s = rep->makespan_s > 0 ? (double)points / rep->makespan_s : 0;
+  rep->mean_batch = sv->launches ? (double)sv->batched_requests /
+                                       (double)(sv->mode == CGX_SERVE_BATCHED ? sv->launches : done)
+                                 : 0;
+  rep->hbm_used = sv->used;
+  return CGX_OK;
+}
+
+int cgx_server_latencies(cgx_server *sv, double *out_ms, int64_t n) {
+  if (!sv || !out_ms) return set_error(CGX_EINVAL, "null argument");
+  std::lock_guard<std::mutex> g(sv->mu);
+  int64_t k = 0;
+  for (const Request &r : sv->reqs) {
+    if (k >= n) break;
+    out_ms[k++] = r.t_done > 0 ? 1e3 * (r.t_done - r.t_arrive) : -1.0;
+  }
+  return CGX_OK;
+}
+
+} // extern "C"

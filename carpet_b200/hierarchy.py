@@ -150,20 +150,22 @@ def build_level(box: Box, parts, ghost: int) -> Level:
     return Level(box[6], box, comps)
 
 
-def nested(nlevels: int, npoints: int, parts=(2, 2, 2), ghost=3, buffer=9, order=5,
+def nested(nlevels: int, npoints, parts=(2, 2, 2), ghost=3, buffer=9, order=5,
            origin=(0, 0, 0)) -> Hierarchy:
-    """``nlevels`` vertex-centred levels of ``npoints``^3 points each, each
-    level covering the central half of the next coarser one."""
-    assert (npoints - 1) % 4 == 0
+    """``nlevels`` vertex-centred levels of ``npoints`` points per axis each
+    (an int or one per axis, each 1 mod 4), each level covering the central
+    half of the next coarser one."""
+    n = (npoints,) * 3 if isinstance(npoints, int) else tuple(npoints)
+    assert all((m - 1) % 4 == 0 for m in n)
     st0 = 2 ** (nlevels - 1)
     lo = list(origin)
     levels = []
     for l in range(nlevels):
         st = st0 >> l
-        box = mkbox(lo, [lo[d] + (npoints - 1) * st for d in range(3)], (st,) * 3)
+        box = mkbox(lo, [lo[d] + (n[d] - 1) * st for d in range(3)], (st,) * 3)
         levels.append(build_level(box, parts, ghost))
-        # next level: the central half, (npoints-1)/4 coarse points in
-        lo = [lo[d] + ((npoints - 1) // 4) * st for d in range(3)]
+        # next level: the central half, (n-1)/4 coarse points in
+        lo = [lo[d] + ((n[d] - 1) // 4) * st for d in range(3)]
     h = Hierarchy(levels, ghost, buffer, order)
     schedule(h)
     return h

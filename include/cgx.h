@@ -146,6 +146,39 @@ int cgx_graph_launch(cgx_graph *g, void *stream);
 int cgx_graph_destroy(cgx_graph *g);
 
 /*
+ * Served form: transfer requests from many independent AMR hierarchies.
+ * NO COUNTERPART IN THE REFERENCE (Carpet runs one hierarchy per job); the
+ * operations served are the reference's (sync, boundary prolongation,
+ * restriction of one level), each defined once from a cgx_batch holding its
+ * box-pairs.  A worker thread continuously batches pending requests -- the
+ * oldest of every hierarchy with nothing on the GPU -- into the persistent
+ * kernel on two alternating launch slots; a hierarchy's requests run one
+ * after another in arrival order.  CGX_SERVE_PLAIN serves one request at a
+ * time through per-box launches (the baseline).  Hierarchies are admitted
+ * against an HBM budget with cgx_server_admit/release.
+ */
+#define CGX_SERVE_BATCHED 0
+#define CGX_SERVE_PLAIN 1
+typedef struct cgx_server cgx_server;
+typedef struct cgx_server_report {
+  int64_t requests, launches, fine_points, hbm_used;
+  double p50_ms, p99_ms, mean_ms, makespan_s, points_per_s, mean_batch;
+} cgx_server_report;
+int cgx_server_create(cgx_server **out, int mode, int64_t hbm_budget_bytes,
+                      int max_pairs, int64_t max_tiles, int64_t max_requests);
+int cgx_server_destroy(cgx_server *s);
+int cgx_server_admit(cgx_server *s, int64_t bytes);   /* CGX_ENOMEM if over budget */
+int cgx_server_release(cgx_server *s, int64_t bytes);
+int cgx_server_define_op(cgx_server *s, int hier, const cgx_batch *pairs, int *op_id);
+int cgx_server_start(cgx_server *s);
+int cgx_server_submit(cgx_server *s, int op_id, int64_t *request_id);
+/* submit op_ids[i] at arrival_s[i] seconds after the call (a load replay) */
+int cgx_server_replay(cgx_server *s, const int *op_ids, const double *arrival_s, int n);
+int cgx_server_drain(cgx_server *s); /* wait until every submitted request is done */
+int cgx_server_stats(cgx_server *s, cgx_server_report *rep);
+int cgx_server_latencies(cgx_server *s, double *out_ms, int64_t n);
+
+/*
  * No-allocation form.  NO COUNTERPART IN THE REFERENCE: CarpetLib has no
  * device path at all; this entry point exists for callers of this library
  * that must not allocate device memory -- code that runs while a CUDA graph
