@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--serve-seconds", type=float, default=1.0)
     return p.parse_args()
 
 
@@ -249,6 +251,54 @@ def cpu_sample(h, ngf, seconds, prefer_ref=True):
     return total / el / 1e9, cores, kind, sample
 
 
+# ----------------------------------------------------------------- served
+def served(seconds: float):
+    """The served ensemble: 64 independent 3-level hierarchies (coarse sizes
+    U{24..64} per axis, 4 grid functions x 3 timelevels, 2 components per
+    level), admitted against a 150 GB HBM budget; Poisson request streams
+    (sync/prolong/restrict 60/25/15) at 1e3, 1e4 and 1e5 requests/s, each
+    served continuously batched and, at the lower rates, through the plain
+    per-box drop-in one request at a time."""
+    import torch
+    from carpet_b200.serve import (SERVE_BATCHED, SERVE_PLAIN, Ensemble, Server, ops_for,
+                                   poisson_trace)
+    out = {"workload": "64 hierarchies x 3 vc levels, coarse U{24..64}^3, 4 GFs x 3 TLs, "
+                       "order-5 prolongation + 3-TL time interpolation; Poisson stream "
+                       "sync/prolong/restrict 60/25/15", "budget_gb": 150, "rates": []}
+    warm = Server(mode=SERVE_BATCHED)
+    ens = Ensemble(warm, nhier=64, size_range=(24, 64), seed=42)
+    plain = Server(mode=SERVE_PLAIN)
+    plain_ops = ens.define(plain)
+    keys, arr = poisson_trace(ens, 1e4, 200, seed=1)   # warm-up: module load, attributes
+    warm.replay(ops_for(ens.ops, keys), arr)
+    warm.drain()
+    plain.replay(ops_for(plain_ops, keys[:50]), arr[:50])
+    plain.drain()
+    plain.close()
+    out["hierarchies"] = len(ens.members)
+    out["hbm_gb"] = round(warm.report()["hbm_used"] / 1e9, 3)
+    for rate in (1e3, 1e4, 1e5):
+        n = int(min(rate * seconds, 20000))
+        keys, arr = poisson_trace(ens, rate, n, seed=int(rate))
+        row = {"rate_per_s": rate, "requests": n}
+        for mode, name in ((SERVE_BATCHED, "batched"), (SERVE_PLAIN, "plain")):
+            if mode == SERVE_PLAIN and rate > 1e4:
+                continue  # the plain drop-in falls behind without bound at 1e5/s
+            sv = Server(mode=mode)
+            op_ids = ens.define(sv)
+            torch.cuda.synchronize()
+            sv.replay(ops_for(op_ids, keys), arr)
+            sv.drain()
+            r = sv.report()
+            row[name] = {"p50_ms": round(r["p50_ms"], 4), "p99_ms": round(r["p99_ms"], 4),
+                         "fine_points_per_s": round(r["points_per_s"], 1),
+                         "launches": r["launches"], "mean_batch": round(r["mean_batch"], 2)}
+            sv.close()
+        out["rates"].append(row)
+    warm.close()
+    return out
+
+
 # ----------------------------------------------------------------- main
 def main():
     args = parse()
@@ -419,6 +469,10 @@ def main():
         cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": cores, "kind": kind,
                "sample": sample}
 
+    serve = None
+    if rank == 0 and not args.no_serve:
+        serve = served(args.serve_seconds)
+
     traffic = None
     prof = os.path.join(ROOT, "profiles", "k_batch_traffic.json")
     if os.path.exists(prof):
@@ -448,7 +502,7 @@ def main():
                          "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
                          "kernel": "k_batch (persistent, all phases)",
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"},
-            "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(), "served": serve,
         }
         print(json.dumps(out))
     for g in graphs:

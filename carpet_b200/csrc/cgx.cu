@@ -77,8 +77,8 @@ unsigned long long reciprocal(int n) {
 
 // Tiles of a descriptor.  Prolongation: ptx fine x (<= PTXMAX) by
 // 2*ptyc-1 fine y by PTZ fine z, the widths balanced over the region so that
-// thin regions get narrow, tall tiles.  Copy and restriction: crows rows
-// (j,k) of about CTARGET points.
+// thin regions get narrow, tall tiles.  Copy and restriction: CTILE
+// consecutive points of the flattened region.
 int kind_tiles(Desc &d) {
   const int kind = d.kind;
   const bool prol = kind == K_PROLONG_VC || kind == K_PROLONG_CC || kind == K_PROLONG_ENO;
@@ -97,11 +97,9 @@ int kind_tiles(Desc &d) {
     d.tiles[2] = (d.n[2] + PTZ - 1) / PTZ;
     for (int k = 0; k < 3; ++k) tot *= d.tiles[k];
   } else {
-    const long long rows = (long long)d.n[1] * d.n[2];
-    if (rows * d.n[0] >= (1LL << 31)) return -1;
-    const int crows = std::max(1, std::min(65535, CTARGET / d.n[0]));
-    d.crows = (unsigned short)crows;
-    d.tiles[0] = (int)((rows + crows - 1) / crows);
+    const long long npts = (long long)d.n[0] * d.n[1] * d.n[2];
+    if (npts >= (1LL << 31)) return -1;
+    d.tiles[0] = (int)((npts + CTILE - 1) / CTILE);
     d.tiles[1] = d.tiles[2] = 1;
     tot = d.tiles[0];
     d.rcp0 = reciprocal(d.n[0]);
@@ -467,13 +465,28 @@ int build(int op, int cent, const cgx_array *dst, const cgx_array *srcs, const d
 int launch_pair(const Desc &d, int ntiles, int fp, int *status, cudaStream_t s) {
   const bool high = d.kind == K_PROLONG_VC && d.order >= 7;
   if (high) return klaunch_pair_hi(fp, d, ntiles, status, s);
+  if (!is_stencil(d.kind))
+    return fp == CGX_FP_FMA ? klaunch_spair_f1(d, ntiles, status, s) : klaunch_spair_f0(d, ntiles, status, s);
   return fp == CGX_FP_FMA ? klaunch_pair_f1(d, ntiles, status, s) : klaunch_pair_f0(d, ntiles, status, s);
 }
 
-int launch_map(int fp, const Desc *d, const int2 *tmap, long long ntiles, unsigned long long *counter,
-               int *status, cudaStream_t s) {
-  return fp == CGX_FP_FMA ? klaunch_map_f1(d, tmap, ntiles, counter, status, s)
-                          : klaunch_map_f0(d, tmap, ntiles, counter, status, s);
+// One persistent kernel per non-empty segment of a tile map, each with its
+// own work counter (counter[i], zero on entry).
+int launch_map(int fp, const Desc *d, const int2 *tmap, const long long seg[NSEG + 1],
+               unsigned long long *counter, int *status, cudaStream_t s) {
+  for (int i = 0; i < NSEG; ++i) {
+    const long long n = seg[i + 1] - seg[i];
+    if (n <= 0) continue;
+    int rc;
+    if (i == 0)
+      rc = fp == CGX_FP_FMA ? klaunch_map_f1(d, tmap, n, counter, status, s)
+                            : klaunch_map_f0(d, tmap, n, counter, status, s);
+    else
+      rc = fp == CGX_FP_FMA ? klaunch_stream_f1(i - 1, d, tmap + seg[i], n, counter + i, status, s)
+                            : klaunch_stream_f0(i - 1, d, tmap + seg[i], n, counter + i, status, s);
+    if (rc) return rc;
+  }
+  return CGX_OK;
 }
 
 } // namespace
@@ -491,8 +504,9 @@ struct cgx_batch {
   size_t tmap_cap = 0;
   int n_uploaded = 0;     // descriptors in the persistent kernel's queue
   long long tiles_uploaded = 0;
+  long long seg[NSEG + 1] = {0}; // the tile map's segments
   std::vector<int> high_idx; // descriptors launched per box
-  unsigned long long *d_counter = nullptr;
+  unsigned long long *d_counter = nullptr; // one per tile-map segment
   int *d_status = nullptr;
   int fp_mode = CGX_FP_EXACT;
 };
@@ -547,7 +561,7 @@ int cgx_copy(int op, int cent, const cgx_array *dst, const cgx_array *src, const
 int cgx_batch_create(cgx_batch **out) {
   if (!out) return fail(CGX_EINVAL, "null batch");
   cgx_batch *b = new cgx_batch();
-  cudaError_t e = cudaMalloc(&b->d_counter, sizeof(unsigned long long));
+  cudaError_t e = cudaMalloc(&b->d_counter, NSEG * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMalloc(&b->d_status, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(b->d_status, 0, sizeof(int));
   if (e != cudaSuccess) {
@@ -611,15 +625,21 @@ int cgx_batch_stats(const cgx_batch *b, int64_t *npairs, int64_t *ntiles, int64_
 int cgx_batch_upload(cgx_batch *b, void *stream) {
   if (!b) return fail(CGX_EINVAL, "null batch");
   cudaStream_t s = (cudaStream_t)stream;
-  // queue order: prolongation tiles (the heaviest) first, then the rest
+  // queue order: by tile-map segment (prolongation, then each streaming
+  // variant); within a segment, largest work per tile first, so that a
+  // persistent kernel's last claims are small ones
   std::vector<int> order;
   b->high_idx.clear();
-  for (int pass = 0; pass < 2; ++pass)
-    for (size_t i = 0; i < b->descs.size(); ++i) {
-      if (b->high[i]) { if (pass == 0) b->high_idx.push_back((int)i); continue; }
-      bool prol = b->descs[i].kind >= K_PROLONG_VC;
-      if ((pass == 0) == prol) order.push_back((int)i);
-    }
+  for (size_t i = 0; i < b->descs.size(); ++i) {
+    if (b->high[i]) b->high_idx.push_back((int)i);
+    else order.push_back((int)i);
+  }
+  auto weight = [&](int i) { return (double)b->points[i] / (double)std::max(1, b->ntiles[i]); };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+    const int sa = segment_of(b->descs[a]), sc = segment_of(b->descs[c]);
+    if (sa != sc) return sa < sc;
+    return weight(a) > weight(c);
+  });
   const size_t n = order.size();
   if (n > b->d_cap) {
     cudaFree(b->d_descs);
@@ -635,11 +655,15 @@ int cgx_batch_upload(cgx_batch *b, void *stream) {
   std::vector<Desc> hd(n);
   std::vector<long long> hp(n);
   long long acc = 0;
+  long long cnt[NSEG] = {0};
   for (size_t i = 0; i < n; ++i) {
     hd[i] = b->descs[order[i]];
     hp[i] = acc;
     acc += b->ntiles[order[i]];
+    cnt[segment_of(hd[i])] += b->ntiles[order[i]];
   }
+  b->seg[0] = 0;
+  for (int i = 0; i < NSEG; ++i) b->seg[i + 1] = b->seg[i] + cnt[i];
   b->n_uploaded = (int)n;
   b->tiles_uploaded = acc;
   b->fp_mode = g_fp_mode;
@@ -670,12 +694,10 @@ int cgx_batch_launch(cgx_batch *b, void *stream) {
   if (!b) return fail(CGX_EINVAL, "null batch");
   cudaStream_t s = (cudaStream_t)stream;
   if (b->n_uploaded > 0) {
-    cudaError_t e = cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), s);
+    cudaError_t e = cudaMemsetAsync(b->d_counter, 0, NSEG * sizeof(unsigned long long), s);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
-    int rc = launch_map(b->fp_mode, b->d_descs, b->d_tmap, b->tiles_uploaded, b->d_counter,
-                        b->d_status, s);
+    int rc = launch_map(b->fp_mode, b->d_descs, b->d_tmap, b->seg, b->d_counter, b->d_status, s);
     if (rc) return rc;
-
   }
   for (int i : b->high_idx) {
     int rc = launch_pair(b->descs[i], b->ntiles[i], b->fp_mode, b->d_status, s);
@@ -887,12 +909,12 @@ int batch_pairs(const cgx_batch *b, const Desc **descs, const int **ntiles, cons
   return CGX_OK;
 }
 
-int launch_tile_map(const Desc *d_descs, const int2 *d_tmap, long long ntiles,
+int launch_tile_map(const Desc *d_descs, const int2 *d_tmap, const long long seg[NSEG + 1],
                     unsigned long long *d_counter, int *d_status, int fp, cudaStream_t s) {
-  if (ntiles <= 0) return CGX_OK;
-  cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), s);
+  if (seg[NSEG] <= 0) return CGX_OK;
+  cudaError_t e = cudaMemsetAsync(d_counter, 0, NSEG * sizeof(unsigned long long), s);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
-  return launch_map(fp, d_descs, d_tmap, ntiles, d_counter, d_status, s);
+  return launch_map(fp, d_descs, d_tmap, seg, d_counter, d_status, s);
 }
 
 int launch_one_pair(const Desc &d, int ntiles, int fp, int *status, cudaStream_t s) {

@@ -39,10 +39,6 @@ constexpr int NWARPS = NTHREADS / 32;
 // descriptor (thin regions get narrow, tall tiles); ptx*ptyc <= NTHREADS,
 // one thread per (fine x, coarse y row) column.
 constexpr int PTXMAX = 30, PTYCMAX = 16, PTZ = 64;
-// copy / restriction: a tile is crows consecutive rows (j,k) of the region,
-// about CTARGET points; CU rows (or packed row groups) per warp are in
-// flight at a time
-constexpr int CTARGET = 16384, CU = 4;
 
 struct Desc {
   int kind, order, ntl, tkind;
@@ -52,7 +48,7 @@ struct Desc {
   int sext[3];  // logical extent of the source arrays (load clamp)
   int tiles[3]; // tile grid over the region
   unsigned char ptx, ptyc; // prolongation tile shape (fine x, coarse y rows)
-  unsigned short crows;    // copy/restriction tile: region rows (j,k) per tile
+  short pad_;
   long long ssy, ssz; // source strides (elements) in y and z
   long long dsy, dsz; // destination strides
   unsigned long long rcp0, rcp1; // ceil(2^64 / n[0]), ceil(2^64 / n[1]); 0 for 1
@@ -238,122 +234,135 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 // start; the restrictions step by 2 in the source.
 //
 // These are pure streaming operations on regions of any shape -- ghost
-// zones are 3 points thin in one direction -- so a tile is a run of region
-// rows, streamed with lanes along x and short rows packed several to a
-// warp access; a row index is split into (j,k) by multiply-high with a
-// precomputed reciprocal.
+// zones are 3 points thin in one direction -- and run in a high-occupancy
+// kernel of their own.  A tile is CTILE consecutive points of the region
+// flattened x-fastest: every lane is busy whatever the shape and
+// consecutive lanes touch consecutive x; each thread loads its CPT points
+// before it stores any.  A flat index is split into (i, j, k) by
+// multiply-high with precomputed reciprocals.
+constexpr int CPT = 8;
+constexpr int CTILE = CPT * NTHREADS;
+
+// The streaming kinds, one persistent kernel each.
+enum StreamVariant : int {
+  SV_COPY1 = 0,       // copy, one timelevel
+  SV_COPY2 = 1,       // copy, linear time interpolation
+  SV_COPY3Q = 2,      // copy, quadratic time interpolation
+  SV_COPY3E = 3,      // copy, ENO time interpolation
+  SV_RESTRICT_VC = 4, // injection
+  SV_RESTRICT_CC = 5, // 8-point average
+  SV_COUNT = 6
+};
+
+template <class D> __host__ __device__ __forceinline__ int stream_variant(const D &d) {
+  if (d.kind == K_RESTRICT_VC) return SV_RESTRICT_VC;
+  if (d.kind == K_RESTRICT_CC) return SV_RESTRICT_CC;
+  if (d.kind != K_COPY) return -1;
+  if (d.ntl == 1) return SV_COPY1;
+  if (d.ntl == 2) return SV_COPY2;
+  return d.tkind == T_ENO ? SV_COPY3E : SV_COPY3Q;
+}
 
 // floor(p / n) for p, n < 2^32 given M = ceil(2^64 / n) (M = 0 for n = 1)
 __device__ __forceinline__ unsigned div_rcp(unsigned p, unsigned long long M) {
   return M ? (unsigned)__umul64hi((unsigned long long)p, M) : p;
 }
 
-// Row-streaming over a tile of the region: every (row, x segment) item is
-// one warp access of up to 32 consecutive x.  Rows shorter than 32 are
-// packed 32/n0 to a warp access.  body_load(item-slot, j, k, i) issues the
-// loads of one point, body_store(item-slot, j, k, i) its store; CU items per
-// warp are loaded before any is stored.
-template <class D, class LoadF, class StoreF>
-__device__ __forceinline__ void stream_rows(D &d, int tile, LoadF &&body_load, StoreF &&body_store) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int n0 = d.n[0], n1 = d.n[1];
-  const unsigned nrows = (unsigned)n1 * d.n[2];
-  const unsigned r0 = (unsigned)tile * d.crows;
-  const unsigned r1 = min(nrows, r0 + d.crows);
-  // segment geometry
-  const bool packed = n0 < 32;
-  const int per = packed ? 32 / n0 : 1;             // rows per item
-  const int nseg = packed ? 1 : (n0 + 31) >> 5;     // items per row
-  const int sub = packed ? lane / n0 : 0;
-  const int li = packed ? lane - sub * n0 : lane;   // x within the segment
-  const unsigned nitems = packed ? (r1 - r0 + per - 1) / per : (r1 - r0) * nseg;
-  for (unsigned it0 = warp; it0 < nitems; it0 += NWARPS * CU) {
-    int jj[CU], kk[CU], ii[CU];
-#pragma unroll
-    for (int u = 0; u < CU; ++u) {
-      const unsigned it = it0 + u * NWARPS;
-      ii[u] = -1;
-      if (it < nitems) {
-        unsigned row;
-        int i;
-        if (packed) {
-          row = r0 + it * per + sub;
-          i = li;
-          if (sub >= per || row >= r1) continue;
-        } else {
-          const unsigned rseg = it / nseg;
-          row = r0 + rseg;
-          i = (int)(it - rseg * nseg) * 32 + li;
-          if (i >= n0) continue;
-        }
-        const unsigned k = div_rcp(row, d.rcp1);
-        jj[u] = (int)(row - k * (unsigned)n1);
-        kk[u] = (int)k;
-        ii[u] = i;
-        body_load(u, jj[u], kk[u], i);
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < CU; ++u)
-      if (ii[u] >= 0) body_store(u, jj[u], kk[u], ii[u]);
-  }
+template <class D>
+__device__ __forceinline__ void unflatten(D &d, unsigned p, int &i, int &j, int &k) {
+  const unsigned q = div_rcp(p, d.rcp0);
+  i = (int)(p - q * (unsigned)d.n[0]);
+  const unsigned r = div_rcp(q, d.rcp1);
+  j = (int)(q - r * (unsigned)d.n[1]);
+  k = (int)r;
 }
 
 template <int FMA, int NTL, int TK, class D>
-__device__ void copy_tile(D &d, int tile) {
-  double v[CU][NTL];
-  stream_rows(
-      d, tile,
-      [&](int u, int j, int k, int i) {
+__device__ __forceinline__ void copy_tile(D &d, int tile) {
+  const unsigned npts = (unsigned)d.n[0] * d.n[1] * d.n[2];
+  const unsigned p0 = (unsigned)tile * CTILE + threadIdx.x;
+  // G points (G x NTL loads) in flight per thread and group
+  constexpr int G = NTL == 1 ? CPT : CPT / 2;
+#pragma unroll
+  for (int r0 = 0; r0 < CPT; r0 += G) {
+    double v[G][NTL];
+#pragma unroll
+    for (int r = 0; r < G; ++r) {
+      const unsigned p = p0 + (r0 + r) * NTHREADS;
+      if (p < npts) {
+        int i, j, k;
+        unflatten(d, p, i, j, k);
         const long long si = (d.soff[0] + i) + (d.soff[1] + j) * d.ssy + (d.soff[2] + k) * d.ssz;
 #pragma unroll
-        for (int t = 0; t < NTL; ++t) v[u][t] = __ldg(d.src[t] + si);
-      },
-      [&](int u, int j, int k, int i) {
+        for (int t = 0; t < NTL; ++t) v[r][t] = __ldg(d.src[t] + si);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < G; ++r) {
+      const unsigned p = p0 + (r0 + r) * NTHREADS;
+      if (p < npts) {
+        int i, j, k;
+        unflatten(d, p, i, j, k);
         d.dst[(d.doff[0] + i) + (d.doff[1] + j) * d.dsy + (d.doff[2] + k) * d.dsz] =
-            tcombine<FMA, TK, NTL>(d.w, v[u]);
-      });
+            tcombine<FMA, TK, NTL>(d.w, v[r]);
+      }
+    }
+  }
 }
 
 template <class D>
-__device__ void restrict_vc_tile(D &d, int tile) {
-  double v[CU];
+__device__ __forceinline__ void restrict_vc_tile(D &d, int tile) {
+  const unsigned npts = (unsigned)d.n[0] * d.n[1] * d.n[2];
+  const unsigned p0 = (unsigned)tile * CTILE + threadIdx.x;
   const double *s = d.src[0];
-  stream_rows(
-      d, tile,
-      [&](int u, int j, int k, int i) {
-        v[u] = __ldg(s + (d.soff[0] + 2 * i) + (d.soff[1] + 2 * j) * d.ssy + (d.soff[2] + 2 * k) * d.ssz);
-      },
-      [&](int u, int j, int k, int i) {
-        d.dst[(d.doff[0] + i) + (d.doff[1] + j) * d.dsy + (d.doff[2] + k) * d.dsz] = v[u];
-      });
+  double v[CPT];
+#pragma unroll
+  for (int r = 0; r < CPT; ++r) {
+    const unsigned p = p0 + r * NTHREADS;
+    if (p < npts) {
+      int i, j, k;
+      unflatten(d, p, i, j, k);
+      v[r] = __ldg(s + (d.soff[0] + 2 * i) + (d.soff[1] + 2 * j) * d.ssy + (d.soff[2] + 2 * k) * d.ssz);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < CPT; ++r) {
+    const unsigned p = p0 + r * NTHREADS;
+    if (p < npts) {
+      int i, j, k;
+      unflatten(d, p, i, j, k);
+      d.dst[(d.doff[0] + i) + (d.doff[1] + j) * d.dsy + (d.doff[2] + k) * d.dsz] = v[r];
+    }
+  }
 }
 
 template <int FMA, class D>
-__device__ void restrict_cc_tile(D &d, int tile) {
-  double v[CU];
+__device__ __forceinline__ void restrict_cc_tile(D &d, int tile) {
+  const unsigned npts = (unsigned)d.n[0] * d.n[1] * d.n[2];
+  const unsigned p0 = (unsigned)tile * CTILE + threadIdx.x;
   const double w = 0.125; // f1*f1*f1 with f1 = f2 = 1/2
-  stream_rows(
-      d, tile,
-      [&](int u, int j, int k, int i) {
-        const double *q = d.src[0] + (d.soff[0] + 2 * i) + (d.soff[1] + 2 * j) * d.ssy +
-                          (d.soff[2] + 2 * k) * d.ssz;
-        const double a0 = __ldg(q), a1 = __ldg(q + 1), a2 = __ldg(q + d.ssy), a3 = __ldg(q + 1 + d.ssy);
-        const double a4 = __ldg(q + d.ssz), a5 = __ldg(q + 1 + d.ssz);
-        const double a6 = __ldg(q + d.ssy + d.ssz), a7 = __ldg(q + 1 + d.ssy + d.ssz);
-        // order of restrict_3d_cc_rf2.cc:253-260
-        double res = mul(w, a0);
-        res = madd<FMA>(w, a1, res);
-        res = madd<FMA>(w, a2, res);
-        res = madd<FMA>(w, a3, res);
-        res = madd<FMA>(w, a4, res);
-        res = madd<FMA>(w, a5, res);
-        res = madd<FMA>(w, a6, res);
-        v[u] = madd<FMA>(w, a7, res);
-      },
-      [&](int u, int j, int k, int i) {
-        d.dst[(d.doff[0] + i) + (d.doff[1] + j) * d.dsy + (d.doff[2] + k) * d.dsz] = v[u];
-      });
+#pragma unroll 2
+  for (int r = 0; r < CPT; ++r) {
+    const unsigned p = p0 + r * NTHREADS;
+    if (p >= npts) break;
+    int i, j, k;
+    unflatten(d, p, i, j, k);
+    const double *q = d.src[0] + (d.soff[0] + 2 * i) + (d.soff[1] + 2 * j) * d.ssy +
+                      (d.soff[2] + 2 * k) * d.ssz;
+    const double a0 = __ldg(q), a1 = __ldg(q + 1), a2 = __ldg(q + d.ssy), a3 = __ldg(q + 1 + d.ssy);
+    const double a4 = __ldg(q + d.ssz), a5 = __ldg(q + 1 + d.ssz);
+    const double a6 = __ldg(q + d.ssy + d.ssz), a7 = __ldg(q + 1 + d.ssy + d.ssz);
+    // order of restrict_3d_cc_rf2.cc:253-260
+    double res = mul(w, a0);
+    res = madd<FMA>(w, a1, res);
+    res = madd<FMA>(w, a2, res);
+    res = madd<FMA>(w, a3, res);
+    res = madd<FMA>(w, a4, res);
+    res = madd<FMA>(w, a5, res);
+    res = madd<FMA>(w, a6, res);
+    res = madd<FMA>(w, a7, res);
+    d.dst[(d.doff[0] + i) + (d.doff[1] + j) * d.dsy + (d.doff[2] + k) * d.dsz] = res;
+  }
 }
 
 // ---------------------------------------------------------------- prolongation

@@ -26,9 +26,15 @@ int host_build(int op, int cent, const cgx_array *dst, const cgx_array *srcs, co
 int batch_pairs(const cgx_batch *b, const Desc **descs, const int **ntiles, const long long **points,
                 int *n);
 
-// Persistent-kernel launch over a device tile map (cgx.cu); grid sized to
-// the device.
-int launch_tile_map(const Desc *d_descs, const int2 *d_tmap, long long ntiles,
+// A tile map is laid out in segments, one persistent kernel each: segment 0
+// holds the prolongation tiles (the stencil kernel), segment 1 + v the
+// tiles of streaming variant v.  seg[i] .. seg[i+1] is segment i's range.
+constexpr int NSEG = 1 + SV_COUNT;
+
+// Persistent-kernel launches over the non-empty segments of a device tile
+// map (cgx.cu); d_counter points to NSEG work counters, which this zeroes;
+// grids sized to the device.
+int launch_tile_map(const Desc *d_descs, const int2 *d_tmap, const long long seg[NSEG + 1],
                     unsigned long long *d_counter, int *d_status, int fp, cudaStream_t s);
 
 // One plain per-box launch (cgx.cu).
@@ -46,6 +52,18 @@ int klaunch_search_f0(const Desc *d, const long long *prefix, int ndesc, long lo
                       unsigned long long *counter, int *status, cudaStream_t s);
 int klaunch_search_f1(const Desc *d, const long long *prefix, int ndesc, long long ntiles,
                       unsigned long long *counter, int *status, cudaStream_t s);
+
+int klaunch_spair_f0(const Desc &d, int ntiles, int *status, cudaStream_t s);
+int klaunch_spair_f1(const Desc &d, int ntiles, int *status, cudaStream_t s);
+int klaunch_stream_f0(int variant, const Desc *d, const int2 *tmap, long long ntiles,
+                      unsigned long long *counter, int *status, cudaStream_t s);
+int klaunch_stream_f1(int variant, const Desc *d, const int2 *tmap, long long ntiles,
+                      unsigned long long *counter, int *status, cudaStream_t s);
+
+// stencil (prolongation) kinds run in the shared-memory kernels, the others
+// in the streaming kernels
+inline bool is_stencil(int kind) { return kind >= K_PROLONG_VC; }
+inline int segment_of(const Desc &d) { return is_stencil(d.kind) ? 0 : 1 + stream_variant(d); }
 
 int current_fp_mode();
 int set_error(int code, const char *fmt, ...);

@@ -14,4 +14,11 @@ int klaunch_search_f0(const Desc *d, const long long *prefix, int ndesc, long lo
                      unsigned long long *counter, int *status, cudaStream_t s) {
   return kern::launch_search_t<0>(d, prefix, ndesc, ntiles, counter, status, s);
 }
+int klaunch_spair_f0(const Desc &d, int ntiles, int *status, cudaStream_t s) {
+  return kern::launch_spair_t<0>(d, ntiles, status, s);
+}
+int klaunch_stream_f0(int variant, const Desc *d, const int2 *tmap, long long ntiles,
+                     unsigned long long *counter, int *status, cudaStream_t s) {
+  return kern::launch_stream_map_t<0>(variant, d, tmap, ntiles, counter, status, s);
+}
 } // namespace cgx

@@ -64,5 +64,37 @@ int launch_search_t(const Desc *d_descs, const long long *d_prefix, int ndesc, l
   return e == cudaSuccess ? CGX_OK : cuda_error(e, "k_batch launch");
 }
 
+template <int FMA> int launch_spair_t(const Desc &d, int ntiles, int *status, cudaStream_t s) {
+  k_spair<FMA><<<ntiles, NTHREADS, 0, s>>>(d, status);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? CGX_OK : cuda_error(e, "k_spair launch");
+}
+
+template <int FMA, int V>
+int launch_stream_v(const Desc *d_descs, const int2 *d_tmap, long long ntiles,
+                    unsigned long long *d_counter, int *d_status, cudaStream_t s) {
+  int grid = 0;
+  persistent_grid(k_stream_map<FMA, V>, 0, ntiles, &grid);
+  k_stream_map<FMA, V><<<grid, NTHREADS, 0, s>>>(d_descs, d_tmap, ntiles, d_counter, d_status);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? CGX_OK : cuda_error(e, "k_stream_map launch");
+}
+
+template <int FMA>
+int launch_stream_map_t(int variant, const Desc *d_descs, const int2 *d_tmap, long long ntiles,
+                        unsigned long long *d_counter, int *d_status, cudaStream_t s) {
+  switch (variant) {
+  case SV_COPY1: return launch_stream_v<FMA, SV_COPY1>(d_descs, d_tmap, ntiles, d_counter, d_status, s);
+  case SV_COPY2: return launch_stream_v<FMA, SV_COPY2>(d_descs, d_tmap, ntiles, d_counter, d_status, s);
+  case SV_COPY3Q: return launch_stream_v<FMA, SV_COPY3Q>(d_descs, d_tmap, ntiles, d_counter, d_status, s);
+  case SV_COPY3E: return launch_stream_v<FMA, SV_COPY3E>(d_descs, d_tmap, ntiles, d_counter, d_status, s);
+  case SV_RESTRICT_VC:
+    return launch_stream_v<FMA, SV_RESTRICT_VC>(d_descs, d_tmap, ntiles, d_counter, d_status, s);
+  case SV_RESTRICT_CC:
+    return launch_stream_v<FMA, SV_RESTRICT_CC>(d_descs, d_tmap, ntiles, d_counter, d_status, s);
+  }
+  return set_error(CGX_EINVAL, "bad streaming variant %d", variant);
+}
+
 } // namespace kern
 } // namespace cgx

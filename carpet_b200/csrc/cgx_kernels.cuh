@@ -192,6 +192,76 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 }
 
 
+// Streaming kernels (copy and restrictions): no shared-memory stage, so
+// they run at high occupancy -- many warps keep enough loads in flight.
+constexpr int STREAM_BLOCKS_PER_SM = 4;
+
+// one streaming variant's tile; V is a StreamVariant
+template <int FMA, int V> __device__ __forceinline__ void stream_tile(const Desc &d, int tile) {
+  if (V == SV_COPY1) copy_tile<FMA, 1, T_NONE>(d, tile);
+  else if (V == SV_COPY2) copy_tile<FMA, 2, T_LIN>(d, tile);
+  else if (V == SV_COPY3Q) copy_tile<FMA, 3, T_QUAD>(d, tile);
+  else if (V == SV_COPY3E) copy_tile<FMA, 3, T_ENO>(d, tile);
+  else if (V == SV_RESTRICT_VC) restrict_vc_tile(d, tile);
+  else restrict_cc_tile<FMA>(d, tile);
+}
+
+// Per-box form: every variant in one dispatch.  The descriptor parameter
+// is uniform, so its fields are read from the parameter space.
+template <int FMA>
+__global__ void __launch_bounds__(NTHREADS, STREAM_BLOCKS_PER_SM)
+    k_spair(const __grid_constant__ Desc d, int *status) {
+  __shared__ __align__(16) Desc s_d;
+  if (threadIdx.x == 0) s_d = d;
+  __syncthreads();
+  switch (stream_variant(s_d)) {
+  case SV_COPY1: stream_tile<FMA, SV_COPY1>(s_d, blockIdx.x); return;
+  case SV_COPY2: stream_tile<FMA, SV_COPY2>(s_d, blockIdx.x); return;
+  case SV_COPY3Q: stream_tile<FMA, SV_COPY3Q>(s_d, blockIdx.x); return;
+  case SV_COPY3E: stream_tile<FMA, SV_COPY3E>(s_d, blockIdx.x); return;
+  case SV_RESTRICT_VC: stream_tile<FMA, SV_RESTRICT_VC>(s_d, blockIdx.x); return;
+  case SV_RESTRICT_CC: stream_tile<FMA, SV_RESTRICT_CC>(s_d, blockIdx.x); return;
+  }
+  if (threadIdx.x == 0) report(status, CGX_EDEVICE);
+}
+
+// Persistent form: one kernel per variant over that variant's segment of
+// the tile map.  The descriptor fields are shared-memory reads that the
+// compiler keeps in registers; one variant per kernel keeps that within the
+// register budget of STREAM_BLOCKS_PER_SM CTAs per SM.
+template <int FMA, int V>
+__global__ void __launch_bounds__(NTHREADS, STREAM_BLOCKS_PER_SM)
+    k_stream_map(const Desc *__restrict__ descs, const int2 *__restrict__ tmap, long long ntiles,
+                 unsigned long long *counter, int *status) {
+  __shared__ long long s_t, s_next;
+  __shared__ int2 s_m;
+  __shared__ __align__(16) Desc s_d;
+  if (threadIdx.x == 0) {
+    const long long t = (long long)atomicAdd(counter, 1ULL);
+    s_t = t;
+    s_m = t < ntiles ? tmap[t] : make_int2(0, 0);
+  }
+  __syncthreads();
+  for (;;) {
+    if (s_t >= ntiles) break;
+    const int2 m = s_m;
+    if (threadIdx.x < sizeof(Desc) / 8)
+      reinterpret_cast<unsigned long long *>(&s_d)[threadIdx.x] =
+          __ldg(reinterpret_cast<const unsigned long long *>(descs + m.x) + threadIdx.x);
+    if (threadIdx.x == 0) s_next = (long long)atomicAdd(counter, 1ULL);
+    __syncthreads();
+    if (stream_variant(s_d) == V) stream_tile<FMA, V>(s_d, m.y);
+    else if (threadIdx.x == 0) report(status, CGX_EDEVICE);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const long long tn = s_next;
+      s_t = tn;
+      s_m = tn < ntiles ? tmap[tn] : make_int2(0, 0);
+    }
+    __syncthreads();
+  }
+}
+
 // dynamic shared memory of the widest variant a kernel dispatches
 inline size_t smem_bytes(bool high) {
   return sizeof(double) * (high ? smem_doubles<11>() : smem_doubles<5>());

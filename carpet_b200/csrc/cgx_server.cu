@@ -98,7 +98,7 @@ int slot_init(Slot &s, size_t desc_cap, size_t tile_cap) {
   if (e == cudaSuccess) e = cudaMallocHost(&s.h_descs, desc_cap * sizeof(Desc));
   if (e == cudaSuccess) e = cudaMalloc(&s.d_tmap, tile_cap * sizeof(int2));
   if (e == cudaSuccess) e = cudaMallocHost(&s.h_tmap, tile_cap * sizeof(int2));
-  if (e == cudaSuccess) e = cudaMalloc(&s.d_counter, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&s.d_counter, NSEG * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMalloc(&s.d_status, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(s.d_status, 0, sizeof(int));
   if (e != cudaSuccess) return cuda_error(e, "server slot allocation");
@@ -169,22 +169,31 @@ bool launch_batch(cgx_server *sv, Slot &s) {
     }
   }
   if (take.empty()) return false;
-  // concatenate descriptors and tile maps in pinned staging
+  // concatenate descriptors in pinned staging, and the tile maps segment
+  // by segment (prolongation tiles of all requests, then each streaming
+  // variant's), one persistent kernel per segment
   size_t di = 0, ti = 0;
   const double t = sv->now();
   for (int r : take) {
     const OpTemplate &op = sv->ops[sv->reqs[r].op];
-    for (size_t k = 0; k < op.descs.size(); ++k) {
-      s.h_descs[di] = op.descs[k];
-      for (int j = 0; j < op.ntiles[k]; ++j) s.h_tmap[ti++] = make_int2((int)di, j);
-      ++di;
-    }
+    for (size_t k = 0; k < op.descs.size(); ++k) s.h_descs[di++] = op.descs[k];
     sv->reqs[r].t_launch = t;
   }
+  long long seg[NSEG + 1];
+  for (int g = 0; g < NSEG; ++g) {
+    seg[g] = (long long)ti;
+    size_t d0 = 0;
+    for (int r : take) {
+      const OpTemplate &op = sv->ops[sv->reqs[r].op];
+      for (size_t k = 0; k < op.descs.size(); ++k, ++d0)
+        if (segment_of(op.descs[k]) == g)
+          for (int j = 0; j < op.ntiles[k]; ++j) s.h_tmap[ti++] = make_int2((int)d0, j);
+    }
+  }
+  seg[NSEG] = (long long)ti;
   cudaMemcpyAsync(s.d_descs, s.h_descs, di * sizeof(Desc), cudaMemcpyHostToDevice, s.stream);
   cudaMemcpyAsync(s.d_tmap, s.h_tmap, ti * sizeof(int2), cudaMemcpyHostToDevice, s.stream);
-  int rc = launch_tile_map(s.d_descs, s.d_tmap, (long long)ti, s.d_counter, s.d_status, sv->fp,
-                           s.stream);
+  int rc = launch_tile_map(s.d_descs, s.d_tmap, seg, s.d_counter, s.d_status, sv->fp, s.stream);
   if (rc) sv->error = rc;
   cudaEventRecord(s.done, s.stream);
   s.reqs = take;

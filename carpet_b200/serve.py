@@ -129,9 +129,17 @@ class Ensemble:
             self.members.append(Member(h, st, nbytes))
         for m, mem in enumerate(self.members):
             fill_random(mem.storage, fill_seed + m)
-            self._define(m, mem)
+        self.ops = self.define(server)
 
-    def _define(self, m: int, mem: Member):
+    def define(self, server: Server) -> Dict[Tuple[int, str, int], int]:
+        """register every (hierarchy, transfer, level) operation with a server;
+        returns the operation ids"""
+        ops: Dict[Tuple[int, str, int], int] = {}
+        for m, mem in enumerate(self.members):
+            self._define(server, ops, m, mem)
+        return ops
+
+    def _define(self, server: Server, ops, m: int, mem: Member):
         h, st = mem.hier, mem.storage
         L = len(h.levels)
         dtc = 1.0 / 64
@@ -143,7 +151,7 @@ class Ensemble:
                 for p in h.sync[l]:
                     b.add(arrs[g][p.dst_comp], [arrs[g][p.src_comp]], [0.0], p.dstbox, p.srcbox,
                           0.0, 1, 0, op=OP_LAGRANGE, cent=VERTEX)
-            self.ops[(m, "sync", l)] = self.server.define(m, b)
+            ops[(m, "sync", l)] = server.define(m, b)
         for l in range(1, L):
             b = Batch()
             dst = st.data[l][0]
@@ -152,7 +160,7 @@ class Ensemble:
                 for p in h.prolong[l]:
                     b.add(dst[g][p.dst_comp], [s[g][p.src_comp] for s in srcs], times, p.dstbox,
                           p.srcbox, -dtc / 2, self.order, 2, op=OP_LAGRANGE, cent=VERTEX)
-            self.ops[(m, "prolong", l)] = self.server.define(m, b)
+            ops[(m, "prolong", l)] = server.define(m, b)
         for l in range(L - 1):
             b = Batch()
             dst, src = st.data[l][0], st.data[l + 1][0]
@@ -160,7 +168,7 @@ class Ensemble:
                 for p in h.restrict[l + 1]:
                     b.add(dst[g][p.dst_comp], [src[g][p.src_comp]], [0.0], p.dstbox, p.srcbox, 0.0,
                           self.order, 0, op=OP_LAGRANGE, cent=VERTEX)
-            self.ops[(m, "restrict", l)] = self.server.define(m, b)
+            ops[(m, "restrict", l)] = server.define(m, b)
 
     def snapshot(self):
         return [[p.clone() for p in lp] for mem in self.members for lp in mem.storage.pools]
@@ -190,7 +198,8 @@ def fill_random(st: Storage, seed: int):
 def poisson_trace(ens: Ensemble, rate: float, n: int, seed=0, mix=(0.60, 0.25, 0.15)):
     """n requests with exponential inter-arrival times at ``rate`` per second:
     sync / prolongation / restriction in proportions ``mix``, a uniformly
-    chosen hierarchy and level."""
+    chosen hierarchy and level.  Returns (keys, arrival times); map keys to a
+    server's operation ids with ``ops_for``."""
     rng = np.random.default_rng(seed)
     arr = np.cumsum(rng.exponential(1.0 / rate, n))
     arr -= arr[0]
@@ -206,5 +215,9 @@ def poisson_trace(ens: Ensemble, rate: float, n: int, seed=0, mix=(0.60, 0.25, 0
             key = (m, "prolong", int(rng.integers(1, L)))
         else:
             key = (m, "restrict", int(rng.integers(0, L - 1)))
-        ops.append(ens.ops[key])
+        ops.append(key)
     return ops, arr
+
+
+def ops_for(op_ids: Dict[Tuple[int, str, int], int], keys):
+    return [op_ids[k] for k in keys]
