@@ -9,6 +9,8 @@
 //
 // Device side: cgx_device.cuh (tile routines) and cgx_kernels.cuh
 // (kernels), launched through cgx_kern_*.cu.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -75,6 +77,16 @@ unsigned long long reciprocal(int n) {
   return (unsigned long long)((one + (unsigned)n - 1) / (unsigned)n);
 }
 
+struct Win { int lo0, hi0, lo1, hi1; };
+Win family_window(int kind, int order) {
+  if (kind == K_PROLONG_VC) { int lo = -((order + 1) / 2) + 1; return {0, 0, lo, lo + order}; }
+  if (kind == K_PROLONG_CC) {
+    int n = order + 1, lo0 = -n / 2, lo1 = -n / 2 + (order % 2 ? 1 : 0);
+    return {lo0, lo0 + n - 1, lo1, lo1 + n - 1};
+  }
+  return {0, 0, -1, 2}; // ENO
+}
+
 // Tiles of a descriptor.  Prolongation: ptx fine x (<= PTXMAX) by
 // 2*ptyc-1 fine y by PTZ fine z, the widths balanced over the region so that
 // thin regions get narrow, tall tiles.  Copy and restriction: CTILE
@@ -92,6 +104,12 @@ int kind_tiles(Desc &d) {
     ptyc = std::min(ptyc, (pty + 2) / 2);
     d.ptx = (unsigned char)ptx;
     d.ptyc = (unsigned char)ptyc;
+    // the tensor-copy box of a tile's coarse plane: all coarse bases of ptx
+    // fine points, the stencil window, and one point of even-alignment shift
+    const Win w = family_window(kind, d.order);
+    const int W = std::max(w.hi0, w.hi1) - std::min(w.lo0, w.lo1);
+    d.bx = (unsigned char)(((ptx + 2) / 2 + W + 2) & ~1);
+    d.by = (unsigned char)(ptyc + W);
     d.tiles[0] = (d.n[0] + ptx - 1) / ptx;
     d.tiles[1] = (d.n[1] + 2 * ptyc - 2) / (2 * ptyc - 1);
     d.tiles[2] = (d.n[2] + PTZ - 1) / PTZ;
@@ -176,16 +194,6 @@ int time_weights(int tk, const double *ts, double t, double *w) {
 }
 
 // Coarse window [lo, hi] of one parity relative to the coarse base c.
-struct Win { int lo0, hi0, lo1, hi1; };
-Win family_window(int kind, int order) {
-  if (kind == K_PROLONG_VC) { int lo = -((order + 1) / 2) + 1; return {0, 0, lo, lo + order}; }
-  if (kind == K_PROLONG_CC) {
-    int n = order + 1, lo0 = -n / 2, lo1 = -n / 2 + (order % 2 ? 1 : 0);
-    return {lo0, lo0 + n - 1, lo1, lo1 + n - 1};
-  }
-  return {0, 0, -1, 2}; // ENO
-}
-
 // Every coarse point any fine point of the region reads: the first two and
 // last two fine points of each axis bound it.  Used for the exact in-bounds
 // check (stricter than the reference's expand() test, which works in fine
@@ -472,21 +480,46 @@ int launch_pair(const Desc &d, int ntiles, int fp, int *status, cudaStream_t s) 
 
 // One persistent kernel per non-empty segment of a tile map, each with its
 // own work counter (counter[i], zero on entry).
-int launch_map(int fp, const Desc *d, const int2 *tmap, const long long seg[NSEG + 1],
-               unsigned long long *counter, int *status, cudaStream_t s) {
+int launch_map(int fp, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
+               const long long seg[NSEG + 1], unsigned long long *counter, int *status, cudaStream_t s) {
+  const bool f = fp == CGX_FP_FMA;
   for (int i = 0; i < NSEG; ++i) {
     const long long n = seg[i + 1] - seg[i];
     if (n <= 0) continue;
+    const int2 *tm = tmap + seg[i];
+    unsigned long long *c = counter + i;
     int rc;
-    if (i == 0)
-      rc = fp == CGX_FP_FMA ? klaunch_map_f1(d, tmap, n, counter, status, s)
-                            : klaunch_map_f0(d, tmap, n, counter, status, s);
-    else
-      rc = fp == CGX_FP_FMA ? klaunch_stream_f1(i - 1, d, tmap + seg[i], n, counter + i, status, s)
-                            : klaunch_stream_f0(i - 1, d, tmap + seg[i], n, counter + i, status, s);
+    if (i < TV_COUNT) {
+      const bool p1 = i / 4 >= 5;
+      rc = f ? (p1 ? klaunch_tma_f1_p1 : klaunch_tma_f1_p0)(i, d, maps, tm, n, c, status, s)
+             : (p1 ? klaunch_tma_f0_p1 : klaunch_tma_f0_p0)(i, d, maps, tm, n, c, status, s);
+    } else if (i == SEG_STENCIL) {
+      rc = f ? klaunch_map_f1(d, tm, n, c, status, s) : klaunch_map_f0(d, tm, n, c, status, s);
+    } else {
+      rc = f ? klaunch_stream_f1(i - SEG_STREAM, d, tm, n, c, status, s)
+             : klaunch_stream_f0(i - SEG_STREAM, d, tm, n, c, status, s);
+    }
     if (rc) return rc;
   }
   return CGX_OK;
+}
+
+// cuTensorMapEncodeTiled from the driver, found once; null without a driver
+PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    else
+      cudaGetLastError();
+  }
+  return fn;
 }
 
 } // namespace
@@ -502,6 +535,7 @@ struct cgx_batch {
   size_t d_cap = 0;
   int2 *d_tmap = nullptr; // (descriptor, local tile) of every queued tile
   size_t tmap_cap = 0;
+  CUtensorMap *d_maps = nullptr; // 3 per queued descriptor (d_cap of them)
   int n_uploaded = 0;     // descriptors in the persistent kernel's queue
   long long tiles_uploaded = 0;
   long long seg[NSEG + 1] = {0}; // the tile map's segments
@@ -578,6 +612,7 @@ int cgx_batch_destroy(cgx_batch *b) {
   cudaFree(b->d_descs);
   cudaFree(b->d_prefix);
   cudaFree(b->d_tmap);
+  cudaFree(b->d_maps);
   cudaFree(b->d_counter);
   cudaFree(b->d_status);
   delete b;
@@ -634,9 +669,14 @@ int cgx_batch_upload(cgx_batch *b, void *stream) {
     if (b->high[i]) b->high_idx.push_back((int)i);
     else order.push_back((int)i);
   }
+  // prolongation descriptors whose arrays TMA can stage get tensor maps
+  std::vector<CUtensorMap> em(3 * b->descs.size());
+  std::vector<Desc> dq(b->descs);
+  for (int i : order)
+    if (is_stencil(dq[i].kind) && !encode_tma_maps(dq[i], &em[3 * (size_t)i])) dq[i].bx = 0;
   auto weight = [&](int i) { return (double)b->points[i] / (double)std::max(1, b->ntiles[i]); };
   std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
-    const int sa = segment_of(b->descs[a]), sc = segment_of(b->descs[c]);
+    const int sa = segment_of(dq[a]), sc = segment_of(dq[c]);
     if (sa != sc) return sa < sc;
     return weight(a) > weight(c);
   });
@@ -644,20 +684,25 @@ int cgx_batch_upload(cgx_batch *b, void *stream) {
   if (n > b->d_cap) {
     cudaFree(b->d_descs);
     cudaFree(b->d_prefix);
+    cudaFree(b->d_maps);
     b->d_descs = nullptr;
     b->d_prefix = nullptr;
+    b->d_maps = nullptr;
     size_t cap = std::max<size_t>(n, 64);
     cudaError_t e = cudaMalloc(&b->d_descs, cap * sizeof(Desc));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_prefix, cap * sizeof(long long));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_maps, 3 * cap * sizeof(CUtensorMap));
     if (e != cudaSuccess) { b->d_cap = 0; return cuda_fail(e, "cudaMalloc"); }
     b->d_cap = cap;
   }
   std::vector<Desc> hd(n);
+  std::vector<CUtensorMap> hm3(3 * n);
   std::vector<long long> hp(n);
   long long acc = 0;
   long long cnt[NSEG] = {0};
   for (size_t i = 0; i < n; ++i) {
-    hd[i] = b->descs[order[i]];
+    hd[i] = dq[order[i]];
+    for (int t = 0; t < 3; ++t) hm3[3 * i + t] = em[3 * (size_t)order[i] + t];
     hp[i] = acc;
     acc += b->ntiles[order[i]];
     cnt[segment_of(hd[i])] += b->ntiles[order[i]];
@@ -684,6 +729,8 @@ int cgx_batch_upload(cgx_batch *b, void *stream) {
       e = cudaMemcpyAsync(b->d_prefix, hp.data(), n * sizeof(long long), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(b->d_tmap, hm.data(), hm.size() * sizeof(int2), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(b->d_maps, hm3.data(), hm3.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s); // host vectors are temporaries
     if (e != cudaSuccess) return cuda_fail(e, "descriptor upload");
   }
@@ -696,7 +743,7 @@ int cgx_batch_launch(cgx_batch *b, void *stream) {
   if (b->n_uploaded > 0) {
     cudaError_t e = cudaMemsetAsync(b->d_counter, 0, NSEG * sizeof(unsigned long long), s);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
-    int rc = launch_map(b->fp_mode, b->d_descs, b->d_tmap, b->seg, b->d_counter, b->d_status, s);
+    int rc = launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, b->seg, b->d_counter, b->d_status, s);
     if (rc) return rc;
   }
   for (int i : b->high_idx) {
@@ -909,12 +956,33 @@ int batch_pairs(const cgx_batch *b, const Desc **descs, const int **ntiles, cons
   return CGX_OK;
 }
 
-int launch_tile_map(const Desc *d_descs, const int2 *d_tmap, const long long seg[NSEG + 1],
-                    unsigned long long *d_counter, int *d_status, int fp, cudaStream_t s) {
+int launch_tile_map(const Desc *d_descs, const CUtensorMap *d_maps, const int2 *d_tmap,
+                    const long long seg[NSEG + 1], unsigned long long *d_counter, int *d_status, int fp,
+                    cudaStream_t s) {
   if (seg[NSEG] <= 0) return CGX_OK;
   cudaError_t e = cudaMemsetAsync(d_counter, 0, NSEG * sizeof(unsigned long long), s);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
-  return launch_map(fp, d_descs, d_tmap, seg, d_counter, d_status, s);
+  return launch_map(fp, d_descs, d_maps, d_tmap, seg, d_counter, d_status, s);
+}
+
+bool encode_tma_maps(const Desc &d, CUtensorMap maps[3]) {
+  if (!is_stencil(d.kind) || d.bx == 0 || (d.kind == K_PROLONG_VC && d.order >= 7)) return false;
+  // row and plane pitches must be multiples of 16 bytes
+  if (d.ssy % 2 || d.ssz % 2 || d.ssz >= (1LL << 37)) return false;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tma_encoder();
+  if (!enc) return false;
+  for (int t = 0; t < d.ntl; ++t) {
+    if (reinterpret_cast<uintptr_t>(d.src[t]) % 16) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)d.sext[0], (cuuint64_t)d.sext[1], (cuuint64_t)d.sext[2]};
+    const cuuint64_t strides[2] = {(cuuint64_t)d.ssy * 8, (cuuint64_t)d.ssz * 8};
+    const cuuint32_t box[3] = {d.bx, d.by, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(&maps[t], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(d.src[t]), dims,
+                     strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return false;
+  }
+  return true;
 }
 
 int launch_one_pair(const Desc &d, int ntiles, int fp, int *status, cudaStream_t s) {

@@ -48,7 +48,7 @@ struct Desc {
   int sext[3];  // logical extent of the source arrays (load clamp)
   int tiles[3]; // tile grid over the region
   unsigned char ptx, ptyc; // prolongation tile shape (fine x, coarse y rows)
-  short pad_;
+  unsigned char bx, by;    // tensor-copy box of a tile's coarse plane; bx = 0: not staged by TMA
   long long ssy, ssz; // source strides (elements) in y and z
   long long dsy, dsz; // destination strides
   unsigned long long rcp0, rcp1; // ceil(2^64 / n[0]), ceil(2^64 / n[1]); 0 for 1

@@ -1,10 +1,12 @@
 // cgx_internal.h -- pieces of the library shared between its translation
 // units (not part of the C-ABI).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "../../include/cgx.h"
 #include "cgx_device.cuh"
+#include "cgx_tma.cuh"
 
 namespace cgx {
 
@@ -26,16 +28,27 @@ int host_build(int op, int cent, const cgx_array *dst, const cgx_array *srcs, co
 int batch_pairs(const cgx_batch *b, const Desc **descs, const int **ntiles, const long long **points,
                 int *n);
 
-// A tile map is laid out in segments, one persistent kernel each: segment 0
-// holds the prolongation tiles (the stencil kernel), segment 1 + v the
-// tiles of streaming variant v.  seg[i] .. seg[i+1] is segment i's range.
-constexpr int NSEG = 1 + SV_COUNT;
+// A tile map is laid out in segments, one persistent kernel each: segment v
+// < TV_COUNT holds the prolongation tiles of TMA variant v, segment
+// SEG_STENCIL the other prolongation tiles (cp.async staging), segment
+// SEG_STREAM + v the tiles of streaming variant v.  seg[i] .. seg[i+1] is
+// segment i's range.
+constexpr int SEG_STENCIL = TV_COUNT;
+constexpr int SEG_STREAM = TV_COUNT + 1;
+constexpr int NSEG = SEG_STREAM + SV_COUNT;
 
 // Persistent-kernel launches over the non-empty segments of a device tile
-// map (cgx.cu); d_counter points to NSEG work counters, which this zeroes;
-// grids sized to the device.
-int launch_tile_map(const Desc *d_descs, const int2 *d_tmap, const long long seg[NSEG + 1],
-                    unsigned long long *d_counter, int *d_status, int fp, cudaStream_t s);
+// map (cgx.cu); d_maps[3 * i + t] is the tensor map of descriptor i's
+// timelevel t (read for segment 0 only); d_counter points to NSEG work
+// counters, which this zeroes; grids sized to the device.
+int launch_tile_map(const Desc *d_descs, const CUtensorMap *d_maps, const int2 *d_tmap,
+                    const long long seg[NSEG + 1], unsigned long long *d_counter, int *d_status, int fp,
+                    cudaStream_t s);
+
+// The tensor maps of a prolongation descriptor's source timelevels (cgx.cu):
+// true when the arrays can be staged by TMA (then maps[0 .. ntl-1] are
+// set), false otherwise.
+bool encode_tma_maps(const Desc &d, CUtensorMap maps[3]);
 
 // One plain per-box launch (cgx.cu).
 int launch_one_pair(const Desc &d, int ntiles, int fp, int *status, cudaStream_t s);
@@ -55,6 +68,16 @@ int klaunch_search_f1(const Desc *d, const long long *prefix, int ndesc, long lo
 
 int klaunch_spair_f0(const Desc &d, int ntiles, int *status, cudaStream_t s);
 int klaunch_spair_f1(const Desc &d, int ntiles, int *status, cudaStream_t s);
+// TMA prolongation kernels: f<mode>_p0 families 0-4 (VC 1/3/5, CC 0/1),
+// _p1 families 5-9 (CC 2-5, ENO); variant = 4 * family + time variant
+int klaunch_tma_f0_p0(int variant, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
+                      long long ntiles, unsigned long long *counter, int *status, cudaStream_t s);
+int klaunch_tma_f0_p1(int variant, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
+                      long long ntiles, unsigned long long *counter, int *status, cudaStream_t s);
+int klaunch_tma_f1_p0(int variant, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
+                      long long ntiles, unsigned long long *counter, int *status, cudaStream_t s);
+int klaunch_tma_f1_p1(int variant, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
+                      long long ntiles, unsigned long long *counter, int *status, cudaStream_t s);
 int klaunch_stream_f0(int variant, const Desc *d, const int2 *tmap, long long ntiles,
                       unsigned long long *counter, int *status, cudaStream_t s);
 int klaunch_stream_f1(int variant, const Desc *d, const int2 *tmap, long long ntiles,
@@ -63,7 +86,11 @@ int klaunch_stream_f1(int variant, const Desc *d, const int2 *tmap, long long nt
 // stencil (prolongation) kinds run in the shared-memory kernels, the others
 // in the streaming kernels
 inline bool is_stencil(int kind) { return kind >= K_PROLONG_VC; }
-inline int segment_of(const Desc &d) { return is_stencil(d.kind) ? 0 : 1 + stream_variant(d); }
+inline int segment_of(const Desc &d) {
+  if (!is_stencil(d.kind)) return SEG_STREAM + stream_variant(d);
+  const int v = d.bx ? tma_variant(d) : -1;
+  return v >= 0 ? v : SEG_STENCIL;
+}
 
 int current_fp_mode();
 int set_error(int code, const char *fmt, ...);

@@ -14,6 +14,7 @@
 #include "../../include/cgx.h"
 #include "cgx_device.cuh"
 #include "cgx_internal.h"
+#include "cgx_tma.cuh"
 
 namespace cgx {
 namespace kern {
@@ -252,6 +253,56 @@ __global__ void __launch_bounds__(NTHREADS, STREAM_BLOCKS_PER_SM)
     __syncthreads();
     if (stream_variant(s_d) == V) stream_tile<FMA, V>(s_d, m.y);
     else if (threadIdx.x == 0) report(status, CGX_EDEVICE);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const long long tn = s_next;
+      s_t = tn;
+      s_m = tn < ntiles ? tmap[tn] : make_int2(0, 0);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- TMA form
+// One persistent kernel per prolongation variant (family, order, time
+// interpolation), so that each gets its own register allocation; maps[3 * i
+// + t] is the tensor map of descriptor i's timelevel t.  The claim loop is
+// that of k_stream_map.
+template <int FMA, class F, int NTL, int TK>
+__global__ void __launch_bounds__(NTHREADS, 2)
+    k_tma_map(const Desc *__restrict__ descs, const CUtensorMap *__restrict__ maps,
+              const int2 *__restrict__ tmap, long long ntiles, unsigned long long *counter, int *status,
+              int variant) {
+  extern __shared__ __align__(128) double smraw[];
+  double *sm = reinterpret_cast<double *>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~(uintptr_t)127);
+  __shared__ long long s_t, s_next;
+  __shared__ int2 s_m;
+  __shared__ __align__(16) Desc s_d;
+  __shared__ __align__(8) uint64_t s_bars[TMA_NB];
+  __shared__ int s_abort;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < TMA_NB; ++i) mbar_init(&s_bars[i], 1);
+    mbar_fence_init();
+    s_abort = 0;
+    const long long t = (long long)atomicAdd(counter, 1ULL);
+    s_t = t;
+    s_m = t < ntiles ? tmap[t] : make_int2(0, 0);
+  }
+  __syncthreads();
+  TmaRing ring{s_bars, &s_abort, 0u};
+  for (;;) {
+    if (s_t >= ntiles) break;
+    const int2 m = s_m;
+    if (threadIdx.x < sizeof(Desc) / 8)
+      reinterpret_cast<unsigned long long *>(&s_d)[threadIdx.x] =
+          __ldg(reinterpret_cast<const unsigned long long *>(descs + m.x) + threadIdx.x);
+    if (threadIdx.x == 0) s_next = (long long)atomicAdd(counter, 1ULL);
+    __syncthreads();
+    if (tma_variant(s_d) == variant) {
+      if (!prolong_tile_tma<F, FMA, NTL, TK>(s_d, maps + 3 * (size_t)m.x, m.y, sm, ring, status)) return;
+    } else if (threadIdx.x == 0) {
+      report(status, CGX_EDEVICE);
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
       const long long tn = s_next;

@@ -43,6 +43,7 @@ using clk = std::chrono::steady_clock;
 struct OpTemplate {
   int hier;
   std::vector<Desc> descs;
+  std::vector<CUtensorMap> maps; // 3 per descriptor (prolongation staged by TMA)
   std::vector<int> ntiles;
   long long tiles = 0, points = 0;
 };
@@ -57,6 +58,7 @@ struct Slot {
   cudaEvent_t done = nullptr;
   Desc *d_descs = nullptr, *h_descs = nullptr;
   int2 *d_tmap = nullptr, *h_tmap = nullptr;
+  CUtensorMap *d_maps = nullptr, *h_maps = nullptr;
   unsigned long long *d_counter = nullptr;
   int *d_status = nullptr;
   size_t desc_cap = 0, tile_cap = 0;
@@ -96,6 +98,8 @@ int slot_init(Slot &s, size_t desc_cap, size_t tile_cap) {
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc(&s.d_descs, desc_cap * sizeof(Desc));
   if (e == cudaSuccess) e = cudaMallocHost(&s.h_descs, desc_cap * sizeof(Desc));
+  if (e == cudaSuccess) e = cudaMalloc(&s.d_maps, 3 * desc_cap * sizeof(CUtensorMap));
+  if (e == cudaSuccess) e = cudaMallocHost(&s.h_maps, 3 * desc_cap * sizeof(CUtensorMap));
   if (e == cudaSuccess) e = cudaMalloc(&s.d_tmap, tile_cap * sizeof(int2));
   if (e == cudaSuccess) e = cudaMallocHost(&s.h_tmap, tile_cap * sizeof(int2));
   if (e == cudaSuccess) e = cudaMalloc(&s.d_counter, NSEG * sizeof(unsigned long long));
@@ -113,6 +117,8 @@ void slot_free(Slot &s) {
   cudaFreeHost(s.h_descs);
   cudaFree(s.d_tmap);
   cudaFreeHost(s.h_tmap);
+  cudaFree(s.d_maps);
+  cudaFreeHost(s.h_maps);
   cudaFree(s.d_counter);
   cudaFree(s.d_status);
   if (s.done) cudaEventDestroy(s.done);
@@ -176,7 +182,10 @@ bool launch_batch(cgx_server *sv, Slot &s) {
   const double t = sv->now();
   for (int r : take) {
     const OpTemplate &op = sv->ops[sv->reqs[r].op];
-    for (size_t k = 0; k < op.descs.size(); ++k) s.h_descs[di++] = op.descs[k];
+    for (size_t k = 0; k < op.descs.size(); ++k) {
+      for (int j = 0; j < 3; ++j) s.h_maps[3 * di + j] = op.maps[3 * k + j];
+      s.h_descs[di++] = op.descs[k];
+    }
     sv->reqs[r].t_launch = t;
   }
   long long seg[NSEG + 1];
@@ -193,7 +202,8 @@ bool launch_batch(cgx_server *sv, Slot &s) {
   seg[NSEG] = (long long)ti;
   cudaMemcpyAsync(s.d_descs, s.h_descs, di * sizeof(Desc), cudaMemcpyHostToDevice, s.stream);
   cudaMemcpyAsync(s.d_tmap, s.h_tmap, ti * sizeof(int2), cudaMemcpyHostToDevice, s.stream);
-  int rc = launch_tile_map(s.d_descs, s.d_tmap, seg, s.d_counter, s.d_status, sv->fp, s.stream);
+  cudaMemcpyAsync(s.d_maps, s.h_maps, 3 * di * sizeof(CUtensorMap), cudaMemcpyHostToDevice, s.stream);
+  int rc = launch_tile_map(s.d_descs, s.d_maps, s.d_tmap, seg, s.d_counter, s.d_status, sv->fp, s.stream);
   if (rc) sv->error = rc;
   cudaEventRecord(s.done, s.stream);
   s.reqs = take;
@@ -341,6 +351,10 @@ int cgx_server_define_op(cgx_server *sv, int hier, const cgx_batch *pairs, int *
   op.hier = hier;
   op.descs.assign(d, d + n);
   op.ntiles.assign(nt, nt + n);
+  op.maps.resize(3 * (size_t)n);
+  for (int i = 0; i < n; ++i)
+    if (is_stencil(op.descs[i].kind) && !encode_tma_maps(op.descs[i], &op.maps[3 * (size_t)i]))
+      op.descs[i].bx = 0;
   for (int i = 0; i < n; ++i) { op.tiles += nt[i]; op.points += pts[i]; }
   if (op.descs.size() > sv->slots[0].desc_cap || (size_t)op.tiles > sv->slots[0].tile_cap)
     return set_error(CGX_EINVAL, "operation larger than a server slot");

@@ -1,0 +1,288 @@
+// cgx_tma.cuh -- prolongation with TMA staging (device code).
+//
+// The same separable x -> y -> z arithmetic as prolong_tile (cgx_device.cuh),
+// organised so that every thread's work is fixed per tile and the plane loop
+// is straight-line code:
+//
+//   * one elected thread stages each coarse plane with one bulk tensor copy
+//     per timelevel (cp.async.bulk.tensor, a box of bx x by coarse points),
+//     completing on an mbarrier per ring slot; boxes may start outside the
+//     array (zero fill), which only masked outputs read;
+//   * the x pass is a flat list of (timelevel, coarse row, coarse base)
+//     items spread over all threads, whatever the tile's shape; each item's
+//     shared-memory offsets are computed once per tile;
+//   * the y/z pass keeps its thread = (fine x, coarse y row) mapping and
+//     register z window; threads without a point compute on clamped
+//     indices and their stores are masked, so no branch diverges.
+//
+// A descriptor is eligible when its source arrays can be described to the
+// tensor-copy unit (16-byte aligned base, even row and plane pitches); the
+// host builds one CUtensorMap per timelevel at upload time.
+#pragma once
+#include <cuda.h>
+
+#include "cgx_device.cuh"
+
+namespace cgx {
+
+template <class F> struct TGeom {
+  static constexpr int W = F::HI - F::LO;
+  // box: up to (PTXMAX + 2) / 2 coarse bases + the window + one point of
+  // even-alignment shift, rounded up to even; by = ptyc + W rows
+  static constexpr int BXMAX = ((PTXMAX + 2) / 2 + W + 2) & ~1;
+  static constexpr int BYMAX = PTYCMAX + W;
+  static constexpr int TLS = (BXMAX * BYMAX + 15) / 16 * 16; // doubles per (slot, timelevel)
+  static constexpr int CY = BYMAX;                            // x-pass rows per timelevel
+  static constexpr int XR = 34;                               // x-pass row pitch
+  static constexpr int Q = W + 1;
+};
+constexpr int TMA_PD = 3;          // planes in flight ahead of the x pass
+constexpr int TMA_NB = TMA_PD + 2; // ring slots
+template <class F, int NTL> struct TSmem {
+  using G = TGeom<F>;
+  static constexpr int coarse = TMA_NB * NTL * G::TLS;
+  static constexpr int xbuf = (NTL * G::CY + 1) * G::XR; // + one row for masked x items
+  static constexpr int total = coarse + 2 * xbuf;        // doubles
+};
+
+// The TMA kernels' variants: family (VC 1/3/5, CC 0-5, ENO) x time
+// interpolation (one timelevel, linear, quadratic, ENO).
+constexpr int TV_FAMILIES = 10;
+constexpr int TV_COUNT = 4 * TV_FAMILIES;
+template <class D> __host__ __device__ __forceinline__ int tma_variant(const D &d) {
+  int f = -1;
+  if (d.kind == K_PROLONG_VC) f = d.order == 1 ? 0 : d.order == 3 ? 1 : d.order == 5 ? 2 : -1;
+  else if (d.kind == K_PROLONG_CC) f = d.order >= 0 && d.order <= 5 ? 3 + d.order : -1;
+  else if (d.kind == K_PROLONG_ENO) f = 9;
+  if (f < 0) return -1;
+  const int tv = d.ntl == 1 ? 0 : d.ntl == 2 ? 1 : d.tkind == T_ENO ? 3 : 2;
+  return 4 * f + tv;
+}
+
+// ---------------------------------------------------------------- PTX
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile("{\n"
+               " .reg .pred p;\n"
+               " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+               " selp.u32 %0, 1, 0, p;\n"
+               "}\n"
+               : "=r"(ok)
+               : "r"(smem_u32(bar)), "r"(parity)
+               : "memory");
+  return ok != 0;
+}
+// Waits for the phase of the given parity; gives up after about 2^31 clock
+// cycles (a second) and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > (1LL << 31)) return false;
+  return true;
+}
+// One box of a 3-d tensor map into shared memory, completing on *bar.
+__device__ __forceinline__ void tma_load_3d(double *dst, const CUtensorMap *map, uint64_t *bar, int x, int y,
+                                            int z) {
+  asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+               " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(smem_u32(dst)),
+               "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// Ring state of one CTA: planes staged so far (plane g uses slot g % NB,
+// whose phase g / NB completes when it lands), and a flag that a wait ran
+// out.  Everything here is uniform over the CTA.
+struct TmaRing {
+  uint64_t *bars; // TMA_NB mbarriers, arrival count 1
+  int *abort;     // shared flag, set when a wait gave up
+  unsigned g;     // planes staged by this CTA before the current tile
+};
+
+// One prolongation tile.  Returns false when a wait gave up (the CTA then
+// stops; the status word holds CGX_EDEVICE).
+template <class F, int FMA, int NTL, int TK>
+__device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ maps, int tile, double *sm,
+                                 TmaRing &ring, int *status) {
+  using G = TGeom<F>;
+  using S = TSmem<F, NTL>;
+  constexpr int LO = F::LO, HI = F::HI, Q = G::Q, NB = TMA_NB, PD = TMA_PD;
+  const int tid = threadIdx.x;
+  const int ptx = d.ptx, ptyc = d.ptyc, pty = 2 * ptyc - 1;
+  const int BX = d.bx, BY = d.by;
+
+  const int tx = tile % d.tiles[0], rr = tile / d.tiles[0];
+  const int ty = rr % d.tiles[1], tz = rr / d.tiles[1];
+  const int fx0 = tx * ptx, fy0 = ty * pty, fz0 = tz * PTZ;
+  const int nfx = min(ptx, d.n[0] - fx0), nfy = min(pty, d.n[1] - fy0), nfz = min(PTZ, d.n[2] - fz0);
+  const int sx0 = d.soff[0] + fx0, sy0 = d.soff[1] + fy0, sz0 = d.soff[2] + fz0;
+  const int c_first = sx0 >> 1, c_last = (sx0 + nfx - 1) >> 1;
+  const int cx0 = c_first + LO;
+  const int bx0 = cx0 & ~1; // box start: an even x coordinate
+  const int xs = cx0 - bx0;
+  const int cy0 = (sy0 >> 1) + LO, cy1 = ((sy0 + nfy - 1) >> 1) + HI;
+  const int cz0 = (sz0 >> 1) + LO, cz1 = ((sz0 + nfz - 1) >> 1) + HI;
+  const int nbx = c_last - c_first + 1, ncy = cy1 - cy0 + 1;
+  const int nplanes = cz1 - cz0 + 1;
+  const int xoff = sx0 - 2 * c_first;
+  const unsigned g0 = ring.g;
+
+  double *coarse = sm;
+  double *xrows = sm + S::coarse;
+
+  int issued = 0; // planes staged so far (elected thread)
+  auto issue = [&](int p) { // elected thread: stage plane p
+    issued = p + 1;
+    const unsigned g = g0 + (unsigned)p;
+    const int slot = (int)(g % NB);
+    mbar_expect_tx(&ring.bars[slot], (unsigned)(NTL * BX * BY * 8));
+#pragma unroll
+    for (int t = 0; t < NTL; ++t)
+      tma_load_3d(coarse + (slot * NTL + t) * G::TLS, maps + t, &ring.bars[slot], bx0, cy0, cz0 + p);
+  };
+
+  // --- x items: (timelevel, row, base) spread over the CTA
+  constexpr int IT = (NTL * G::CY * 16 + NTHREADS - 1) / NTHREADS;
+  const int per_t = ncy * nbx, count = NTL * per_t;
+  int xsrc[IT], xdst[IT];
+#pragma unroll
+  for (int k = 0; k < IT; ++k) {
+    const int it = tid + k * NTHREADS;
+    if (it < count) {
+      const int t = it / per_t, rem = it - t * per_t;
+      const int r = rem / nbx, b = rem - r * nbx;
+      xsrc[k] = t * G::TLS + r * BX + xs + b; // window element j of base b at xsrc + j - LO
+      xdst[k] = (t * G::CY + r) * G::XR + 2 * b;
+    } else {
+      xsrc[k] = 0;
+      xdst[k] = NTL * G::CY * G::XR; // the spare row
+    }
+  }
+  auto xpass = [&](int slot, double *__restrict__ xr) {
+    const double *__restrict__ cs = coarse + slot * NTL * G::TLS - LO;
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+      if (k * NTHREADS < count) { // uniform
+        const double *row = cs + xsrc[k];
+        auto get = [&](int m) { return row[m]; };
+        const double xe = F::template first<FMA>(0, get);
+        const double xo = F::template first<FMA>(1, get);
+        *reinterpret_cast<double2 *>(xr + xdst[k]) = make_double2(xe, xo);
+      }
+    }
+  };
+
+  // --- y/z owner: thread = (fine x, coarse y row)
+  const int nthr = ptx * ptyc;
+  const bool tact = tid < nthr;
+  const int my_fx = tact ? tid % ptx : 0, my_cyr = tact ? tid / ptx : 0;
+  const bool wact = (tid & ~31) < nthr; // warp holds an owner
+  const int my_cy = (sy0 >> 1) + my_cyr;
+  const int ys0 = 2 * my_cy;
+  const bool xin = tact && my_fx < nfx;
+  const bool v0 = xin && ys0 >= sy0 && ys0 < sy0 + nfy;
+  const bool v1 = xin && ys0 + 1 >= sy0 && ys0 + 1 < sy0 + nfy;
+  const int ycol = (my_cyr - LO) * G::XR + my_fx + xoff;
+  const long long dsy = d.dsy, dsz = d.dsz;
+  double *const obase = d.dst + (d.doff[0] + fx0 + my_fx) + (long long)(d.doff[1] + fy0 + ys0 - sy0) * dsy +
+                        (long long)(d.doff[2] + fz0 - sz0) * dsz;
+  double w[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) w[k] = (NTL == 1 || (TK != T_ENO && k >= NTL)) ? 0.0 : d.w[k];
+
+  double yq[NTL][2][Q];
+#pragma unroll
+  for (int t = 0; t < NTL; ++t)
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int q = 0; q < Q; ++q) yq[t][h][q] = 0.0;
+
+  auto yzpass = [&](auto Ut, int p, const double *__restrict__ xr) {
+    constexpr int U = decltype(Ut)::value;
+    if (!wact) return; // warp-uniform
+#pragma unroll
+    for (int t = 0; t < NTL; ++t) {
+      const double *col = xr + t * G::CY * G::XR + ycol;
+      auto get = [&](int m) { return col[m * G::XR]; };
+      yq[t][0][U] = F::template next<FMA>(0, get);
+      yq[t][1][U] = F::template next<FMA>(1, get);
+    }
+    const int cb = cz0 + p - HI;
+#pragma unroll
+    for (int zp = 0; zp < 2; ++zp) {
+      const int zs = 2 * cb + zp;
+      const bool zok = zs >= sz0 && zs < sz0 + nfz; // uniform
+      double *o = obase + (long long)zs * dsz;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        double v[NTL];
+#pragma unroll
+        for (int t = 0; t < NTL; ++t)
+          v[t] = F::template next<FMA>(zp, [&](int m) { return yq[t][h][(U + 1 + (m - LO)) % Q]; });
+        const double r = tcombine<FMA, TK, NTL>(w, v);
+        if (zok && (h ? v1 : v0)) o[h ? dsy : 0] = r;
+      }
+    }
+  };
+
+  // Pipeline as in prolong_tile, one barrier per plane; the elected thread
+  // stages plane i + PD at the start of iteration i, into the slot last read
+  // by the x pass of plane i + PD - NB = i - 2.
+  if (tid == 0) {
+#pragma unroll
+    for (int p = 0; p < PD; ++p)
+      if (p < nplanes) issue(p);
+  }
+  bool ok = true;
+  auto iteration = [&](auto Ut, int i) {
+    if (tid == 0 && i + PD < nplanes) issue(i + PD);
+    if (i < nplanes) {
+      const unsigned g = g0 + (unsigned)i;
+      if (!mbar_wait_bounded(&ring.bars[g % NB], (g / NB) & 1)) *ring.abort = 1;
+    }
+    __syncthreads();
+    if (*ring.abort) { ok = false; return; }
+    if (i < nplanes) xpass((int)((g0 + (unsigned)i) % NB), xrows + (i & 1) * S::xbuf);
+    if (i >= 1) yzpass(Ut, i - 1, xrows + ((i - 1) & 1) * S::xbuf);
+  };
+  iteration(std::integral_constant<int, Q - 1>(), 0);
+  for (int i0 = 1; ok && i0 <= nplanes; i0 += Q) {
+    static_for<Q>([&](auto Ut) {
+      constexpr int u = decltype(Ut)::value;
+      const int i = i0 + u;
+      if (ok && i <= nplanes) iteration(std::integral_constant<int, u>(), i);
+    });
+  }
+  if (!ok) {
+    // a wait gave up: wait (bounded) for every plane staged, so that no
+    // copy lands after the CTA has left
+    if (tid == 0) {
+      if (status) atomicCAS(status, 0, CGX_EDEVICE);
+      for (int i = 0; i < issued; ++i) {
+        const unsigned g = g0 + (unsigned)i;
+        mbar_wait_bounded(&ring.bars[g % NB], (g / NB) & 1);
+      }
+    }
+    __syncthreads();
+    return false;
+  }
+  ring.g = g0 + (unsigned)nplanes;
+  __syncthreads(); // shared memory free for the next tile
+  return true;
+}
+
+} // namespace cgx

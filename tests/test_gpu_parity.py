@@ -32,8 +32,20 @@ def bits_equal(a, b):
                           np.ascontiguousarray(b).view(np.uint64))
 
 
-def to_dev(cb, a, bbox):
-    return cb.Data(bbox, torch.from_numpy(a.copy()).cuda())
+def to_dev(cb, a, bbox, pad=False):
+    """a device copy of a; pad=True gives the array an even, NaN-filled row
+    pitch (the layout the TMA-staged prolongation kernels accept)"""
+    if not pad or a.shape[2] % 2 == 0:
+        return cb.Data(bbox, torch.from_numpy(a.copy()).cuda())
+    full = np.full(a.shape[:2] + (a.shape[2] + 1,), np.nan)
+    full[:, :, :a.shape[2]] = a
+    return cb.Data(bbox, torch.from_numpy(full).cuda())
+
+
+# per_box: cgx_transfer; batch: a one-pair batch on arrays of exact shape
+# (TMA-staged when the row pitch is even, cp.async-staged otherwise);
+# batch_pad: a batch on arrays padded to an even pitch (TMA-staged)
+FORMS = ["per_box", "batch", "batch_pad"]
 
 
 def timeset(rng, ntl):
@@ -46,16 +58,17 @@ def timeset(rng, ntl):
     return times, float(rng.uniform(lo + 1e-3, times[0] - 1e-3)), ntl - 1
 
 
-def run_pair(cb, port, c, op, cent, order, ntl, fma, rng, batch=False):
+def run_pair(cb, port, c, op, cent, order, ntl, fma, rng, form="per_box"):
     times, time, ot = timeset(rng, ntl)
     srcs_np = [c["src"], c["src"] * 0.5 + 0.25, c["src"] * -1.5 + 1.0]
     want = c["dst"].copy()
     port.transfer(op, cent, want, c["dstbbox"], srcs_np, c["srcbbox"], times, c["reg"],
                   c["srcbbox"], time, order, ot, fma=fma)
-    dst = to_dev(cb, c["dst"], c["dstbbox"])
-    srcs = [to_dev(cb, s, c["srcbbox"]) for s in srcs_np]
+    pad = form == "batch_pad"
+    dst = to_dev(cb, c["dst"], c["dstbbox"], pad)
+    srcs = [to_dev(cb, s, c["srcbbox"], pad) for s in srcs_np]
     cb.set_fp_mode(fma)
-    if batch:
+    if form != "per_box":
         b = cb.Batch()
         b.add(dst, srcs, times, c["reg"], c["srcbbox"], time, order, ot, op=op, cent=cent)
         b.upload()
@@ -65,60 +78,64 @@ def run_pair(cb, port, c, op, cent, order, ntl, fma, rng, batch=False):
         cb.transfer_data(dst, srcs, times, c["reg"], c["srcbbox"], time, order, ot, op=op,
                          cent=cent)
     torch.cuda.synchronize()
-    got = dst.tensor.cpu().numpy()
+    got = dst.tensor.cpu().numpy()[:, :, :want.shape[2]]
     return got, want
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("fma", [False, True], ids=["exact", "fma"])
 @pytest.mark.parametrize("ntl", [1, 2, 3])
 @pytest.mark.parametrize("order", [1, 3, 5, 7, 9, 11])
-def test_vc_lagrange(cgx, port, order, ntl, fma):
+def test_vc_lagrange(cgx, port, order, ntl, fma, form):
     rng = np.random.default_rng(1000 + 10 * order + ntl)
     for it in range(6):
         big = it >= 4
         c = cases.vc_prolong_case(rng, order, fine_stride=int(rng.choice([1, 2])),
                                   max_ext=40 if big else 9,
                                   kind=("normal", "mixed")[it % 2])
-        got, want = run_pair(cgx, port, c, OP_LAGRANGE, VERTEX, order, ntl, fma, rng)
+        got, want = run_pair(cgx, port, c, OP_LAGRANGE, VERTEX, order, ntl, fma, rng, form)
         assert bits_equal(got, want), np.nanmax(np.abs(got - want))
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("fma", [False, True], ids=["exact", "fma"])
 @pytest.mark.parametrize("ntl", [1, 2, 3])
 @pytest.mark.parametrize("order", [0, 1, 2, 3, 4, 5])
-def test_cc_lagrange(cgx, port, order, ntl, fma):
+def test_cc_lagrange(cgx, port, order, ntl, fma, form):
     rng = np.random.default_rng(2000 + 10 * order + ntl)
     for it in range(5):
         c = cases.cc_prolong_case(rng, order, half=int(rng.choice([1, 2])),
                                   max_ext=36 if it == 4 else 9,
                                   kind=("normal", "mixed")[it % 2])
-        got, want = run_pair(cgx, port, c, OP_LAGRANGE, CELL, order, ntl, fma, rng)
+        got, want = run_pair(cgx, port, c, OP_LAGRANGE, CELL, order, ntl, fma, rng, form)
         assert bits_equal(got, want)
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("fma", [False, True], ids=["exact", "fma"])
 @pytest.mark.parametrize("ntl", [1, 2, 3])
-def test_vc_eno(cgx, port, ntl, fma):
+def test_vc_eno(cgx, port, ntl, fma, form):
     rng = np.random.default_rng(3000 + ntl)
     for it in range(8):
         c = cases.vc_prolong_case(rng, 3, reach=(1, 2), max_ext=40 if it == 7 else 9,
                                   kind=("normal", "steps", "mixed")[it % 3])
-        got, want = run_pair(cgx, port, c, OP_ENO, VERTEX, 3, ntl, fma, rng)
+        got, want = run_pair(cgx, port, c, OP_ENO, VERTEX, 3, ntl, fma, rng, form)
         assert bits_equal(got, want)
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("fma", [False, True], ids=["exact", "fma"])
-def test_restrict_and_copy(cgx, port, fma):
+def test_restrict_and_copy(cgx, port, fma, form):
     rng = np.random.default_rng(4000)
     for it in range(10):
         big = it == 9
         for maker, cent in ((cases.vc_restrict_case, VERTEX), (cases.cc_restrict_case, CELL)):
             c = maker(rng, max_ext=40 if big else 9, kind="mixed")
-            got, want = run_pair(cgx, port, c, OP_LAGRANGE, cent, 1, 1, fma, rng)
+            got, want = run_pair(cgx, port, c, OP_LAGRANGE, cent, 1, 1, fma, rng, form)
             assert bits_equal(got, want)
         c = cases.copy_case(rng, max_ext=40 if big else 9, kind="mixed")
         for ntl in (1, 2, 3):
-            got, want = run_pair(cgx, port, c, OP_LAGRANGE, VERTEX, 1, ntl, fma, rng)
+            got, want = run_pair(cgx, port, c, OP_LAGRANGE, VERTEX, 1, ntl, fma, rng, form)
             assert bits_equal(got, want)
 
 
