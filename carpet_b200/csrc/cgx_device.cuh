@@ -33,12 +33,12 @@ enum TKind : int { T_NONE = 0, T_LIN = 1, T_QUAD = 2, T_ENO = 3 };
 // Tile geometry.
 constexpr int NTHREADS = 256;
 constexpr int NWARPS = NTHREADS / 32;
-// prolongation: a tile is ptx fine x (at most PTXMAX, so at most 16 coarse
+// prolongation: a tile is ptx fine x (at most PTXMAX, so at most 9 coarse
 // bases) by 2*ptyc-1 fine y (at most ptyc coarse rows) by a PTZ chunk of fine
 // z that the CTA marches plane by plane.  ptx and ptyc are chosen per
-// descriptor (thin regions get narrow, tall tiles); ptx*ptyc <= NTHREADS,
-// one thread per (fine x, coarse y row) column.
-constexpr int PTXMAX = 30, PTYCMAX = 16, PTZ = 64;
+// descriptor, balanced over the region; ptx*ptyc <= NTHREADS, one thread per
+// (fine x, coarse y row) column.
+constexpr int PTXMAX = 16, PTYCMAX = 16, PTZ = 64;
 
 struct Desc {
   int kind, order, ntl, tkind;

@@ -274,7 +274,10 @@ __global__ void __launch_bounds__(NTHREADS, 2)
               const int2 *__restrict__ tmap, long long ntiles, unsigned long long *counter, int *status,
               int variant) {
   extern __shared__ __align__(128) double smraw[];
-  double *sm = reinterpret_cast<double *>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~(uintptr_t)127);
+  // 128-byte aligned start, derived from smraw so that the compiler keeps
+  // every access in the shared address space
+  const unsigned sbase = smem_u32(smraw);
+  double *sm = smraw + ((((sbase + 127u) & ~127u) - sbase) >> 3);
   __shared__ long long s_t, s_next;
   __shared__ int2 s_m;
   __shared__ __align__(16) Desc s_d;

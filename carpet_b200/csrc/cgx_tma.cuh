@@ -33,7 +33,10 @@ template <class F> struct TGeom {
   static constexpr int BYMAX = PTYCMAX + W;
   static constexpr int TLS = (BXMAX * BYMAX + 15) / 16 * 16; // doubles per (slot, timelevel)
   static constexpr int CY = BYMAX;                            // x-pass rows per timelevel
-  static constexpr int XR = 34;                               // x-pass row pitch
+  // x-pass row pitch: two fine points per coarse base; the y pass's lane
+  // (row i / 16, column i % 16) then reads word i modulo 16, so a
+  // half-warp's 8-byte loads meet no bank conflict
+  static constexpr int XR = 2 * PTXMAX;
   static constexpr int Q = W + 1;
 };
 constexpr int TMA_PD = 3;          // planes in flight ahead of the x pass
@@ -123,6 +126,7 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
   const int tid = threadIdx.x;
   const int ptx = d.ptx, ptyc = d.ptyc, pty = 2 * ptyc - 1;
   const int BX = d.bx, BY = d.by;
+  constexpr int XR = G::XR;
 
   const int tx = tile % d.tiles[0], rr = tile / d.tiles[0];
   const int ty = rr % d.tiles[1], tz = rr / d.tiles[1];
@@ -155,7 +159,7 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
   };
 
   // --- x items: (timelevel, row, base) spread over the CTA
-  constexpr int IT = (NTL * G::CY * 16 + NTHREADS - 1) / NTHREADS;
+  constexpr int IT = (NTL * G::CY * ((PTXMAX + 2) / 2) + NTHREADS - 1) / NTHREADS; // nbx <= 9
   const int per_t = ncy * nbx, count = NTL * per_t;
   int xsrc[IT], xdst[IT];
 #pragma unroll
@@ -165,10 +169,10 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
       const int t = it / per_t, rem = it - t * per_t;
       const int r = rem / nbx, b = rem - r * nbx;
       xsrc[k] = t * G::TLS + r * BX + xs + b; // window element j of base b at xsrc + j - LO
-      xdst[k] = (t * G::CY + r) * G::XR + 2 * b;
+      xdst[k] = (t * G::CY + r) * XR + 2 * b;
     } else {
       xsrc[k] = 0;
-      xdst[k] = NTL * G::CY * G::XR; // the spare row
+      xdst[k] = NTL * G::CY * XR; // the spare row
     }
   }
   auto xpass = [&](int slot, double *__restrict__ xr) {
@@ -185,17 +189,17 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
     }
   };
 
-  // --- y/z owner: thread = (fine x, coarse y row)
-  const int nthr = ptx * ptyc;
-  const bool tact = tid < nthr;
-  const int my_fx = tact ? tid % ptx : 0, my_cyr = tact ? tid / ptx : 0;
-  const bool wact = (tid & ~31) < nthr; // warp holds an owner
+  // --- y/z owner: thread = (fine x, coarse y row) = (tid % 16, tid / 16)
+  static_assert(PTXMAX == 16 && NTHREADS == 16 * PTYCMAX, "y/z thread layout");
+  const int my_fx = tid & 15, my_cyr = tid >> 4;
+  const bool tact = my_fx < ptx && my_cyr < ptyc;
+  const bool wact = 2 * (tid >> 5) < ptyc; // warp holds an owner
   const int my_cy = (sy0 >> 1) + my_cyr;
   const int ys0 = 2 * my_cy;
   const bool xin = tact && my_fx < nfx;
   const bool v0 = xin && ys0 >= sy0 && ys0 < sy0 + nfy;
   const bool v1 = xin && ys0 + 1 >= sy0 && ys0 + 1 < sy0 + nfy;
-  const int ycol = (my_cyr - LO) * G::XR + my_fx + xoff;
+  const int ycol = (my_cyr - LO) * XR + my_fx + xoff;
   const long long dsy = d.dsy, dsz = d.dsz;
   double *const obase = d.dst + (d.doff[0] + fx0 + my_fx) + (long long)(d.doff[1] + fy0 + ys0 - sy0) * dsy +
                         (long long)(d.doff[2] + fz0 - sz0) * dsz;
@@ -216,8 +220,8 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
     if (!wact) return; // warp-uniform
 #pragma unroll
     for (int t = 0; t < NTL; ++t) {
-      const double *col = xr + t * G::CY * G::XR + ycol;
-      auto get = [&](int m) { return col[m * G::XR]; };
+      const double *col = xr + t * G::CY * XR + ycol;
+      auto get = [&](int m) { return col[m * XR]; };
       yq[t][0][U] = F::template next<FMA>(0, get);
       yq[t][1][U] = F::template next<FMA>(1, get);
     }
