@@ -16,7 +16,8 @@ e2e          the same step through the public API with the grid data in
              pinned host memory: H2D of every array the step reads and D2H of
              every array it writes, inside the timed region
 plain        the plain per-box form (one launch per box-pair), same step
-roofline     the persistent kernel's algorithmic bytes / its CUDA-event time
+roofline     the dominant kernel (the phase kind with the largest share of
+             the step): its algorithmic bytes per launch / its CUDA-event time
 cpu_baseline CarpetLib's own operators (compiled from the reference) on the
              host cores, a bounded sample of the same step
 
@@ -41,6 +42,15 @@ WORKLOAD = "5 vc levels x 129^3 (2x2x2 comps), 25 GFs x 3 TLs, ghost 3, buffer 9
            "one coarse Berger-Oliger step"
 
 
+# the kernel each phase kind of the step runs (batches are homogeneous)
+PHASE_KERNELS = {
+    ("prolong", 3): "k_tma_map<VC<5>, 3 TL quadratic> (prolongation + time interpolation)",
+    ("prolong", 1): "k_tma_map<VC<5>, 1 TL> (prolongation)",
+    ("restrict", 1): "k_stream_map<injection> (restriction)",
+    ("sync", 1): "k_stream_map<copy, 1 TL> (ghost sync)",
+}
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -62,58 +72,95 @@ def parse():
 
 # ----------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi clock/throttle samples while the timed region runs"""
+    """SM clock and clock-event (throttle) reasons, sampled every 10 ms by a
+    thread through NVML while the timed region runs (nvidia-smi every 200 ms
+    when NVML is not importable).  Reads only; changes no GPU setting."""
 
-    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, index=0):
-        self.index, self.proc, self.lines = index, None, []
+    def __init__(self, torch_device=0):
+        self.dev, self.samples, self.smax, self.stop = torch_device, [], None, False
+        self.proc = self.t = None
+
+    def _handle(self, nv):
+        import torch
+        try:
+            p = torch.cuda.get_device_properties(self.dev)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.dev)
+
+    def _nvml_loop(self, nv, h):
+        while not self.stop:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                self.samples.append((float(sm), int(r)))
+            except Exception:
+                pass
+            time.sleep(0.01)
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._handle(nv)
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.t = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
             self.t.start()
-        except FileNotFoundError:
-            self.proc = None
+        except Exception:
+            self._smi()
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _smi(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.sw_power_cap,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except FileNotFoundError:
+            self.proc = None
+            return
+        bits = [0x4, 0x8, 0x20, 0x40]
+
+        def read():
+            for line in self.proc.stdout:
+                f = [x.strip() for x in line.split(",")]
+                try:
+                    sm, self.smax = float(f[0]), float(f[1])
+                except (ValueError, IndexError):
+                    continue
+                r = sum(b for b, v in zip(bits, f[2:6]) if v.lower() == "active")
+                self.samples.append((sm, r))
+        self.t = threading.Thread(target=read, daemon=True)
+        self.t.start()
 
     def __exit__(self, *a):
+        self.stop = True
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        if self.t:
+            self.t.join(timeout=5)
 
     def summary(self):
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
-            f = [x.strip() for x in l.split(",")]
-            if len(f) < 7:
-                continue
-            try:
-                sm.append(float(f[0]))
-                smax = float(f[1])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[3:7]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        if not sm:
+        if not self.samples:
             return None
-        sm.sort()
-        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons),
+        sm = sorted(s for s, _ in self.samples)
+        reasons = set()
+        for _, r in self.samples:
+            for bit, name in self.REASONS.items():
+                if r & bit:
+                    reasons.add(name)
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": self.smax, "reasons": sorted(reasons),
                 "samples": len(sm)}
 
 
@@ -349,7 +396,7 @@ def main():
     stats = [bo.stats(k) for k in steps3]
     bytes_step = sum(s["bytes"] for s in stats) / 3
     points_step = sum(s["points"] for s in stats) / 3
-    launches_step = sum(s["launches"] for s in stats) / 3
+    kernels_step = sum(s["kernels"] for s in stats) / 3
     stream = torch.cuda.Stream()
     torch.cuda.synchronize()
 
@@ -371,7 +418,7 @@ def main():
         graphs[s % 3].launch(stream)
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+    with ClockSampler(torch.cuda.current_device()) as clk:
         e0.record(stream)
         for s in range(args.steps):
             graphs[(args.warmup + s) % 3].launch(stream)
@@ -388,7 +435,9 @@ def main():
     value = bytes_step * world / (ms * 1e-3) / 1e9
     fine_pts = points_step * world / (ms * 1e-3)
 
-    # per-launch timing of the persistent kernel (same stream, no graph)
+    # per-launch timing of every phase (same stream, no graph): each phase
+    # is a homogeneous batch, i.e. one kernel; the dominant kernel is the
+    # phase kind with the largest share of the step
     keys = steps3[(args.warmup + args.steps) % 3]
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in keys]
@@ -397,15 +446,27 @@ def main():
         bo.batch(k).launch(stream)
         b_.record(stream)
     stream.synchronize()
-    kt = sum(a.elapsed_time(b_) for a, b_ in evs) * 1e-3
-    kbytes = sum(bo.batch(k).stats()["bytes"] for k in keys)
+    phases = {}
+    for (a, b_), k in zip(evs, keys):
+        name = PHASE_KERNELS[(k[0], k[3])]
+        e = phases.setdefault(name, {"launches": 0, "ms": 0.0, "bytes": 0})
+        e["launches"] += 1
+        e["ms"] += a.elapsed_time(b_)
+        e["bytes"] += bo.batch(k).stats()["bytes"]
+    tot_ms = sum(e["ms"] for e in phases.values())
+    for e in phases.values():
+        e["gbs"] = round(e["bytes"] / (e["ms"] * 1e-3) / 1e9, 1)
+        e["share"] = round(e["ms"] / tot_ms, 3)
+        e["ms"] = round(e["ms"], 3)
+    dom = max(phases, key=lambda n: phases[n]["ms"])
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except OSError:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    achieved = kbytes / kt / 1e9
+    achieved = phases[dom]["gbs"]
+    bytes_per_launch = phases[dom]["bytes"] / phases[dom]["launches"]
 
     # plain per-box form: one launch per box-pair, same step
     plain = None
@@ -473,13 +534,16 @@ def main():
     if rank == 0 and not args.no_serve:
         serve = served(args.serve_seconds)
 
+    # DRAM bytes per launch of the dominant kernel: the ratio of DRAM bytes
+    # to algorithmic bytes that ncu measured on a smaller capture of the same
+    # kernel (profiles/traffic.json), scaled to this launch
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "k_batch_traffic.json")
-    if os.path.exists(prof):
-        try:
-            traffic = json.load(open(prof)).get("bytes_per_launch_scaled")
-        except (OSError, ValueError):
-            traffic = None
+    try:
+        ratios = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        if dom in ratios:
+            traffic = int(ratios[dom]["dram_per_algorithmic_byte"] * bytes_per_launch)
+    except (OSError, ValueError, KeyError):
+        traffic = None
 
     if rank == 0:
         out = {
@@ -497,11 +561,13 @@ def main():
             "pct_nominal_8tbs": round(100 * value / world / 8000.0, 2),
             "plain": plain,
             "batched_vs_plain": None if not plain else round(value / world / plain["value"], 2),
-            "gpu_launches": int(launches_step * args.steps),
+            "gpu_launches": int(round(kernels_step * args.steps)),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-                         "kernel": "k_batch (persistent, all phases)",
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"},
+                         "kernel": dom, "algorithmic_bytes_per_launch": int(bytes_per_launch),
+                         "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks
+                         else "fallback 6650 GB/s"},
+            "phases": phases,
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(), "served": serve,
         }
         print(json.dumps(out))

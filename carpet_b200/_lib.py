@@ -50,6 +50,7 @@ for fn in ("cgx_batch_destroy", "cgx_batch_clear"):
 for fn in ("cgx_batch_upload", "cgx_batch_launch", "cgx_batch_launch_per_box", "cgx_batch_check"):
     getattr(lib, fn).argtypes = [C.c_void_p, C.c_void_p]
 lib.cgx_batch_stats.argtypes = [C.c_void_p] + [_P(C.c_int64)] * 4
+lib.cgx_batch_kernels.argtypes = [C.c_void_p, _P(C.c_int)]
 lib.cgx_graph_begin.argtypes = [C.c_void_p]
 lib.cgx_graph_end.argtypes = [C.c_void_p, _P(C.c_void_p)]
 lib.cgx_graph_launch.argtypes = [C.c_void_p, C.c_void_p]

@@ -207,10 +207,14 @@ class BergerOliger:
                 b.launch(stream)
 
     def stats(self, keys):
-        tot = dict(pairs=0, tiles=0, points=0, bytes=0, launches=0)
+        """totals over the phases: box-pairs, tiles, points, algorithmic
+        bytes, batches (phases) and kernel launches"""
+        tot = dict(pairs=0, tiles=0, points=0, bytes=0, launches=0, kernels=0)
         for k in keys:
-            s = self.batch(k).stats()
+            b = self.batch(k)
+            s = b.stats()
             for n in ("pairs", "tiles", "points", "bytes"):
                 tot[n] += s[n]
             tot["launches"] += 1
+            tot["kernels"] += b.kernels()
         return tot

@@ -753,6 +753,15 @@ int cgx_batch_launch(cgx_batch *b, void *stream) {
   return CGX_OK;
 }
 
+int cgx_batch_kernels(const cgx_batch *b, int *nkernels) {
+  if (!b || !nkernels) return fail(CGX_EINVAL, "null batch");
+  int n = (int)b->high_idx.size();
+  if (b->n_uploaded > 0)
+    for (int i = 0; i < NSEG; ++i) n += b->seg[i + 1] > b->seg[i];
+  *nkernels = n;
+  return CGX_OK;
+}
+
 int cgx_batch_launch_per_box(cgx_batch *b, void *stream) {
   if (!b) return fail(CGX_EINVAL, "null batch");
   for (size_t i = 0; i < b->descs.size(); ++i) {

@@ -148,6 +148,12 @@ class Batch:
         check(lib.cgx_batch_stats(self.h, *[C.byref(x) for x in v]))
         return dict(pairs=v[0].value, tiles=v[1].value, points=v[2].value, bytes=v[3].value)
 
+    def kernels(self) -> int:
+        """kernels one launch() issues for the current upload"""
+        n = C.c_int()
+        check(lib.cgx_batch_kernels(self.h, C.byref(n)))
+        return n.value
+
     def upload(self, stream=None):
         check(lib.cgx_batch_upload(self.h, _stream(stream)))
 

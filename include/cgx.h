@@ -127,8 +127,13 @@ int cgx_batch_stats(const cgx_batch *b, int64_t *npairs, int64_t *ntiles,
                     int64_t *dst_points, int64_t *bytes);
 /* copy descriptors to the device (once per schedule; graph-safe after) */
 int cgx_batch_upload(cgx_batch *b, void *stream);
-/* one persistent-kernel launch over every uploaded box-pair */
+/* the uploaded box-pairs, one persistent kernel per kind of tile (a
+ * homogeneous batch -- one operator, order and timelevel count -- is one
+ * kernel) */
 int cgx_batch_launch(cgx_batch *b, void *stream);
+/* kernels one cgx_batch_launch issues for the current upload (no
+ * counterpart in the reference: a measurement aid) */
+int cgx_batch_kernels(const cgx_batch *b, int *nkernels);
 /* plain per-box launches of the same descriptors (one kernel per pair) */
 int cgx_batch_launch_per_box(cgx_batch *b, void *stream);
 /* device status word of the last launches: 0 or a CGX_E* code */
