@@ -67,6 +67,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--serve-seconds", type=float, default=1.0)
+    p.add_argument("--no-tune", action="store_true", help="default tile configurations")
     return p.parse_args()
 
 
@@ -393,6 +394,12 @@ def main():
     for keys in steps3:
         for k in keys:
             bo.batch(k)
+    tuned = {}
+    if not args.no_tune:
+        for keys in steps3:
+            for k, v in bo.autotune(keys, reps=2).items():
+                if v:
+                    tuned[f"{k[0]}-ntl{k[3]}"] = v
     stats = [bo.stats(k) for k in steps3]
     bytes_step = sum(s["bytes"] for s in stats) / 3
     points_step = sum(s["points"] for s in stats) / 3
@@ -555,7 +562,8 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (~10 GB per step)",
                        "bytes_per_step": int(bytes_step), "fine_points_per_step": int(points_step),
-                       "resident_gb": round(st.nbytes() / 1e9, 2)},
+                       "resident_gb": round(st.nbytes() / 1e9, 2),
+                       "tile_configs": {n: sorted(set(v.values())) for n, v in tuned.items()}},
             "fine_points_per_s": round(fine_pts, 1),
             "pct_hbm_roof": round(100 * value / world / peak, 2),
             "pct_nominal_8tbs": round(100 * value / world / 8000.0, 2),

@@ -51,6 +51,8 @@ for fn in ("cgx_batch_upload", "cgx_batch_launch", "cgx_batch_launch_per_box", "
     getattr(lib, fn).argtypes = [C.c_void_p, C.c_void_p]
 lib.cgx_batch_stats.argtypes = [C.c_void_p] + [_P(C.c_int64)] * 4
 lib.cgx_batch_kernels.argtypes = [C.c_void_p, _P(C.c_int)]
+lib.cgx_batch_autotune.argtypes = [C.c_void_p, C.c_int, C.c_void_p, _P(C.c_int)]
+lib.cgx_batch_set_config.argtypes = [C.c_void_p, C.c_int, C.c_int]
 lib.cgx_graph_begin.argtypes = [C.c_void_p]
 lib.cgx_graph_end.argtypes = [C.c_void_p, _P(C.c_void_p)]
 lib.cgx_graph_launch.argtypes = [C.c_void_p, C.c_void_p]

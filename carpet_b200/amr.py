@@ -198,6 +198,11 @@ class BergerOliger:
                     keys.append(("sync", l, (self.rot[l],), 1))
         return keys
 
+    def autotune(self, keys, reps=2, stream=None):
+        """tile configurations of every phase's prolongation kernels, chosen
+        by timing (runs the phases); returns {phase: {variant: config}}"""
+        return {k: self.batch(k).autotune(reps, stream) for k in dict.fromkeys(keys)}
+
     def run(self, keys, stream=None, per_box=False):
         for k in keys:
             b = self.batch(k)

@@ -70,11 +70,19 @@ struct Box {
   }
 };
 
-// ceil(2^64 / n) for the device's multiply-high division; 0 encodes n = 1
-unsigned long long reciprocal(int n) {
-  if (n <= 1) return 0;
-  const unsigned __int128 one = (unsigned __int128)1 << 64;
-  return (unsigned long long)((one + (unsigned)n - 1) / (unsigned)n);
+// The magic number and shift of div_magic (cgx_device.cuh) for divisor n:
+// l = ceil(log2 n), m = ceil(2^(31+l) / n), s = l - 1; m = 0 encodes n = 1.
+void division_magic(int n, unsigned *m, int *s) {
+  if (n <= 1) {
+    *m = 0;
+    *s = 0;
+    return;
+  }
+  int l = 0;
+  while ((1LL << l) < n) ++l;
+  const unsigned long long num = 1ULL << (31 + l); // l <= 31
+  *m = (unsigned)((num + (unsigned)n - 1) / (unsigned)n);
+  *s = l - 1;
 }
 
 struct Win { int lo0, hi0, lo1, hi1; };
@@ -87,18 +95,15 @@ Win family_window(int kind, int order) {
   return {0, 0, -1, 2}; // ENO
 }
 
-// Tiles of a descriptor.  Prolongation: ptx fine x (<= PTXMAX) by
-// 2*ptyc-1 fine y by PTZ fine z, the widths balanced over the region so that
-// thin regions get narrow, tall tiles.  Copy and restriction: CTILE
-// consecutive points of the flattened region.
-int kind_tiles(Desc &d) {
+// Prolongation tiles: ptx fine x (<= PTXMAX) by 2*ptyc-1 fine y (ptyc <=
+// pycmax coarse rows) by pz fine z, the widths balanced over the region.
+long long prolong_tiles(Desc &d, int pycmax, int pz) {
   const int kind = d.kind;
-  const bool prol = kind == K_PROLONG_VC || kind == K_PROLONG_CC || kind == K_PROLONG_ENO;
   long long tot = 1;
-  if (prol) {
+  {
     const int ntx = (d.n[0] + PTXMAX - 1) / PTXMAX;
     const int ptx = (d.n[0] + ntx - 1) / ntx;
-    int ptyc = std::min(PTYCMAX, NTHREADS / ptx);
+    int ptyc = std::min(pycmax, NTHREADS / ptx);
     const int nty = (d.n[1] + 2 * ptyc - 2) / (2 * ptyc - 1);
     const int pty = (d.n[1] + nty - 1) / nty;
     ptyc = std::min(ptyc, (pty + 2) / 2);
@@ -112,16 +117,29 @@ int kind_tiles(Desc &d) {
     d.by = (unsigned char)(ptyc + W);
     d.tiles[0] = (d.n[0] + ptx - 1) / ptx;
     d.tiles[1] = (d.n[1] + 2 * ptyc - 2) / (2 * ptyc - 1);
-    d.tiles[2] = (d.n[2] + PTZ - 1) / PTZ;
+    d.tiles[2] = (d.n[2] + pz - 1) / pz;
     for (int k = 0; k < 3; ++k) tot *= d.tiles[k];
+  }
+  return tot;
+}
+
+// Tiles of a descriptor.  Prolongation: the default configuration of
+// prolong_tiles (PTYCMAX rows, PTZ fine z).  Copy and restriction: STILE
+// consecutive points of the flattened region.
+int kind_tiles(Desc &d) {
+  const int kind = d.kind;
+  const bool prol = kind == K_PROLONG_VC || kind == K_PROLONG_CC || kind == K_PROLONG_ENO;
+  long long tot = 1;
+  if (prol) {
+    tot = prolong_tiles(d, PTYCMAX, PTZ);
   } else {
     const long long npts = (long long)d.n[0] * d.n[1] * d.n[2];
     if (npts >= (1LL << 31)) return -1;
-    d.tiles[0] = (int)((npts + CTILE - 1) / CTILE);
+    d.tiles[0] = (int)((npts + STILE - 1) / STILE);
     d.tiles[1] = d.tiles[2] = 1;
     tot = d.tiles[0];
-    d.rcp0 = reciprocal(d.n[0]);
-    d.rcp1 = reciprocal(d.n[1]);
+    division_magic(d.n[0], &d.mg[0], &d.sh[0]);
+    division_magic(d.n[1], &d.mg[1], &d.sh[1]);
   }
   return tot > 0x7fffffff ? -1 : (int)tot;
 }
@@ -480,8 +498,18 @@ int launch_pair(const Desc &d, int ntiles, int fp, int *status, cudaStream_t s) 
 
 // One persistent kernel per non-empty segment of a tile map, each with its
 // own work counter (counter[i], zero on entry).
+// the TMA kernels' launchers, [fused][family part][configuration]
+using TmaLaunch = int (*)(int, const Desc *, const CUtensorMap *, const int2 *, long long,
+                          unsigned long long *, int *, cudaStream_t);
+const TmaLaunch kTmaLaunch[2][2][TMA_NCFG] = {
+    {{klaunch_tma_f0_p0_c0, klaunch_tma_f0_p0_c1, klaunch_tma_f0_p0_c2},
+     {klaunch_tma_f0_p1_c0, klaunch_tma_f0_p1_c1, klaunch_tma_f0_p1_c2}},
+    {{klaunch_tma_f1_p0_c0, klaunch_tma_f1_p0_c1, klaunch_tma_f1_p0_c2},
+     {klaunch_tma_f1_p1_c0, klaunch_tma_f1_p1_c1, klaunch_tma_f1_p1_c2}}};
+
 int launch_map(int fp, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
-               const long long seg[NSEG + 1], unsigned long long *counter, int *status, cudaStream_t s) {
+               const long long seg[NSEG + 1], const int *cfg, unsigned long long *counter, int *status,
+               cudaStream_t s) {
   const bool f = fp == CGX_FP_FMA;
   for (int i = 0; i < NSEG; ++i) {
     const long long n = seg[i + 1] - seg[i];
@@ -490,9 +518,9 @@ int launch_map(int fp, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
     unsigned long long *c = counter + i;
     int rc;
     if (i < TV_COUNT) {
-      const bool p1 = i / 4 >= 5;
-      rc = f ? (p1 ? klaunch_tma_f1_p1 : klaunch_tma_f1_p0)(i, d, maps, tm, n, c, status, s)
-             : (p1 ? klaunch_tma_f0_p1 : klaunch_tma_f0_p0)(i, d, maps, tm, n, c, status, s);
+      const int k = cfg ? cfg[i] : 0;
+      if (k < 0 || k >= TMA_NCFG) return fail(CGX_EINVAL, "bad tile configuration %d", k);
+      rc = kTmaLaunch[f][i / 4 >= 5][k](i, d, maps, tm, n, c, status, s);
     } else if (i == SEG_STENCIL) {
       rc = f ? klaunch_map_f1(d, tm, n, c, status, s) : klaunch_map_f0(d, tm, n, c, status, s);
     } else {
@@ -539,6 +567,7 @@ struct cgx_batch {
   int n_uploaded = 0;     // descriptors in the persistent kernel's queue
   long long tiles_uploaded = 0;
   long long seg[NSEG + 1] = {0}; // the tile map's segments
+  int tma_cfg[TV_COUNT] = {0};    // tile configuration of each TMA variant
   std::vector<int> high_idx; // descriptors launched per box
   unsigned long long *d_counter = nullptr; // one per tile-map segment
   int *d_status = nullptr;
@@ -669,12 +698,28 @@ int cgx_batch_upload(cgx_batch *b, void *stream) {
     if (b->high[i]) b->high_idx.push_back((int)i);
     else order.push_back((int)i);
   }
-  // prolongation descriptors whose arrays TMA can stage get tensor maps
+  // prolongation descriptors whose arrays TMA can stage are tiled in their
+  // variant's configuration and get tensor maps
   std::vector<CUtensorMap> em(3 * b->descs.size());
   std::vector<Desc> dq(b->descs);
-  for (int i : order)
-    if (is_stencil(dq[i].kind) && !encode_tma_maps(dq[i], &em[3 * (size_t)i])) dq[i].bx = 0;
-  auto weight = [&](int i) { return (double)b->points[i] / (double)std::max(1, b->ntiles[i]); };
+  std::vector<long long> ntq(b->ntiles.begin(), b->ntiles.end());
+  for (int i : order) {
+    if (!is_stencil(dq[i].kind)) continue;
+    const int v = tma_variant(dq[i]);
+    Desc t = dq[i];
+    long long nt = 0;
+    if (v >= 0) {
+      const TmaCfg &c = TMA_CFGS[b->tma_cfg[v]];
+      nt = prolong_tiles(t, c.pyc, c.pz);
+    }
+    if (v >= 0 && nt > 0 && nt < (1LL << 31) && encode_tma_maps(t, &em[3 * (size_t)i])) {
+      dq[i] = t;
+      ntq[i] = nt;
+    } else {
+      dq[i].bx = 0;
+    }
+  }
+  auto weight = [&](int i) { return (double)b->points[i] / (double)std::max(1LL, ntq[i]); };
   std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
     const int sa = segment_of(dq[a]), sc = segment_of(dq[c]);
     if (sa != sc) return sa < sc;
@@ -704,8 +749,8 @@ int cgx_batch_upload(cgx_batch *b, void *stream) {
     hd[i] = dq[order[i]];
     for (int t = 0; t < 3; ++t) hm3[3 * i + t] = em[3 * (size_t)order[i] + t];
     hp[i] = acc;
-    acc += b->ntiles[order[i]];
-    cnt[segment_of(hd[i])] += b->ntiles[order[i]];
+    acc += ntq[order[i]];
+    cnt[segment_of(hd[i])] += ntq[order[i]];
   }
   b->seg[0] = 0;
   for (int i = 0; i < NSEG; ++i) b->seg[i + 1] = b->seg[i] + cnt[i];
@@ -722,7 +767,7 @@ int cgx_batch_upload(cgx_batch *b, void *stream) {
   }
   std::vector<int2> hm((size_t)acc);
   for (size_t i = 0; i < n; ++i)
-    for (int k = 0; k < b->ntiles[order[i]]; ++k) hm[(size_t)hp[i] + k] = make_int2((int)i, k);
+    for (long long k = 0; k < ntq[order[i]]; ++k) hm[(size_t)hp[i] + k] = make_int2((int)i, (int)k);
   if (n) {
     cudaError_t e = cudaMemcpyAsync(b->d_descs, hd.data(), n * sizeof(Desc), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
@@ -743,13 +788,78 @@ int cgx_batch_launch(cgx_batch *b, void *stream) {
   if (b->n_uploaded > 0) {
     cudaError_t e = cudaMemsetAsync(b->d_counter, 0, NSEG * sizeof(unsigned long long), s);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
-    int rc = launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, b->seg, b->d_counter, b->d_status, s);
+    int rc = launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, b->seg, b->tma_cfg, b->d_counter,
+                        b->d_status, s);
     if (rc) return rc;
   }
   for (int i : b->high_idx) {
     int rc = launch_pair(b->descs[i], b->ntiles[i], b->fp_mode, b->d_status, s);
     if (rc) return rc;
   }
+  return CGX_OK;
+}
+
+// The autotuner: for every TMA prolongation variant present, run its
+// segment of the batch in each tile configuration (one untimed launch, then
+// `reps` timed with events on the stream) and keep the fastest; then upload
+// with the choices.  Repeated launches of a batch write the same values
+// (pairs write disjoint points and read none of them), so tuning on the
+// caller's own data is safe.
+static_assert(CGX_TMA_VARIANTS == TV_COUNT && CGX_TMA_CONFIGS == TMA_NCFG, "tuning constants of the C-ABI");
+int cgx_batch_autotune(cgx_batch *b, int reps, void *stream, int *chosen) {
+  if (!b || reps < 1) return fail(CGX_EINVAL, "autotune: bad arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = cgx_batch_upload(b, stream);
+  if (rc) return rc;
+  bool present[TV_COUNT];
+  for (int v = 0; v < TV_COUNT; ++v) present[v] = b->seg[v + 1] > b->seg[v];
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
+  auto run_segment = [&](int v) {
+    long long sg[NSEG + 1];
+    for (int i = 0; i <= NSEG; ++i) sg[i] = i <= v ? b->seg[v] : b->seg[v + 1];
+    cudaError_t m = cudaMemsetAsync(b->d_counter, 0, NSEG * sizeof(unsigned long long), s);
+    if (m != cudaSuccess) return cuda_fail(m, "cudaMemsetAsync");
+    return launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, sg, b->tma_cfg, b->d_counter,
+                      b->d_status, s);
+  };
+  for (int v = 0; v < TV_COUNT && rc == CGX_OK; ++v) {
+    if (!present[v]) continue;
+    int best = 0;
+    float best_ms = 0.f;
+    for (int c = 0; c < TMA_NCFG && rc == CGX_OK; ++c) {
+      b->tma_cfg[v] = c;
+      if ((rc = cgx_batch_upload(b, stream))) break;
+      if ((rc = run_segment(v))) break;
+      e = cudaEventRecord(e0, s);
+      for (int r = 0; r < reps && rc == CGX_OK && e == cudaSuccess; ++r) rc = run_segment(v);
+      if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e != cudaSuccess) rc = cuda_fail(e, "autotune timing");
+      if (rc == CGX_OK && (c == 0 || ms < best_ms)) {
+        best = c;
+        best_ms = ms;
+      }
+    }
+    b->tma_cfg[v] = best;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  if (chosen)
+    for (int v = 0; v < TV_COUNT; ++v) chosen[v] = present[v] ? b->tma_cfg[v] : -1;
+  return cgx_batch_upload(b, stream);
+}
+
+int cgx_batch_set_config(cgx_batch *b, int variant, int config) {
+  if (!b || variant < -1 || variant >= TV_COUNT || config < 0 || config >= TMA_NCFG)
+    return fail(CGX_EINVAL, "set_config: variant %d / configuration %d out of range", variant, config);
+  for (int v = 0; v < TV_COUNT; ++v)
+    if (variant < 0 || v == variant) b->tma_cfg[v] = config;
   return CGX_OK;
 }
 
@@ -971,7 +1081,7 @@ int launch_tile_map(const Desc *d_descs, const CUtensorMap *d_maps, const int2 *
   if (seg[NSEG] <= 0) return CGX_OK;
   cudaError_t e = cudaMemsetAsync(d_counter, 0, NSEG * sizeof(unsigned long long), s);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
-  return launch_map(fp, d_descs, d_maps, d_tmap, seg, d_counter, d_status, s);
+  return launch_map(fp, d_descs, d_maps, d_tmap, seg, nullptr, d_counter, d_status, s);
 }
 
 bool encode_tma_maps(const Desc &d, CUtensorMap maps[3]) {

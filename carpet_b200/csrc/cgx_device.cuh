@@ -51,7 +51,8 @@ struct Desc {
   unsigned char bx, by;    // tensor-copy box of a tile's coarse plane; bx = 0: not staged by TMA
   long long ssy, ssz; // source strides (elements) in y and z
   long long dsy, dsz; // destination strides
-  unsigned long long rcp0, rcp1; // ceil(2^64 / n[0]), ceil(2^64 / n[1]); 0 for 1
+  unsigned mg[2]; // streaming kinds: division magic for n[0], n[1] (div_magic)
+  int sh[2];
   const double *src[3];
   double *dst;
   double w[8]; // time weights (layout of the oracle's cgxo_time_weights)
@@ -234,14 +235,12 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 // start; the restrictions step by 2 in the source.
 //
 // These are pure streaming operations on regions of any shape -- ghost
-// zones are 3 points thin in one direction -- and run in a high-occupancy
-// kernel of their own.  A tile is CTILE consecutive points of the region
-// flattened x-fastest: every lane is busy whatever the shape and
-// consecutive lanes touch consecutive x; each thread loads its CPT points
-// before it stores any.  A flat index is split into (i, j, k) by
-// multiply-high with precomputed reciprocals.
-constexpr int CPT = 8;
-constexpr int CTILE = CPT * NTHREADS;
+// zones are 3 points thin in one direction.  A tile is STILE consecutive
+// points of the region flattened x-fastest, run by the LANES threads of a
+// CTA: every lane is busy whatever the shape, consecutive lanes touch
+// consecutive x, and each thread issues a group of loads before its stores.  A flat index is split into (i, j, k) by
+// 32-bit multiply-high with precomputed magic numbers.
+constexpr int STILE = 2048;
 
 // The streaming kinds, one persistent kernel each.
 enum StreamVariant : int {
@@ -263,95 +262,117 @@ template <class D> __host__ __device__ __forceinline__ int stream_variant(const 
   return d.tkind == T_ENO ? SV_COPY3E : SV_COPY3Q;
 }
 
-// floor(p / n) for p, n < 2^32 given M = ceil(2^64 / n) (M = 0 for n = 1)
-__device__ __forceinline__ unsigned div_rcp(unsigned p, unsigned long long M) {
-  return M ? (unsigned)__umul64hi((unsigned long long)p, M) : p;
+// floor(p / n) for 0 <= p < 2^31 (Granlund & Montgomery, "Division by
+// invariant integers using multiplication", 1994, theorem 4.2 with N = 31):
+// with l = ceil(log2 n), m = ceil(2^(31+l) / n) < 2^32 and s = l - 1,
+// floor(p / n) = umulhi(p, m) >> s; m = 0 encodes n = 1.
+__device__ __forceinline__ unsigned div_magic(unsigned p, unsigned m, int s) {
+  return m ? (__umulhi(p, m) >> s) : p;
 }
 
 template <class D>
-__device__ __forceinline__ void unflatten(D &d, unsigned p, int &i, int &j, int &k) {
-  const unsigned q = div_rcp(p, d.rcp0);
+__device__ __forceinline__ void unflatten(const D &d, unsigned p, int &i, int &j, int &k) {
+  const unsigned q = div_magic(p, d.mg[0], d.sh[0]);
   i = (int)(p - q * (unsigned)d.n[0]);
-  const unsigned r = div_rcp(q, d.rcp1);
+  const unsigned r = div_magic(q, d.mg[1], d.sh[1]);
   j = (int)(q - r * (unsigned)d.n[1]);
   k = (int)r;
 }
 
-template <int FMA, int NTL, int TK, class D>
-__device__ __forceinline__ void copy_tile(D &d, int tile) {
+// group sizes: points whose loads a thread issues before it stores them
+template <int LANES, int NTL> __host__ __device__ constexpr int stream_group() {
+  return (STILE / LANES) < (NTL == 1 ? 8 : 4) ? (STILE / LANES) : (NTL == 1 ? 8 : 4);
+}
+
+template <int FMA, int NTL, int TK, int LANES, class D>
+__device__ __forceinline__ void copy_tile(const D &d, int tile, int lid) {
+  // ENO time interpolation holds more per point: smaller groups
+  constexpr int PER = STILE / LANES, G = stream_group<LANES, NTL>() / (TK == T_ENO ? 2 : 1);
   const unsigned npts = (unsigned)d.n[0] * d.n[1] * d.n[2];
-  const unsigned p0 = (unsigned)tile * CTILE + threadIdx.x;
-  // G points (G x NTL loads) in flight per thread and group
-  constexpr int G = NTL == 1 ? CPT : CPT / 2;
+  const unsigned p0 = (unsigned)tile * STILE + lid;
+  const double *src[NTL];
 #pragma unroll
-  for (int r0 = 0; r0 < CPT; r0 += G) {
+  for (int t = 0; t < NTL; ++t) src[t] = d.src[t] + (d.soff[0] + d.soff[1] * d.ssy + d.soff[2] * d.ssz);
+  double *dst = d.dst + (d.doff[0] + d.doff[1] * d.dsy + d.doff[2] * d.dsz);
+  double w[NTL == 1 ? 1 : 8];
+#pragma unroll
+  for (int k = 0; k < (NTL == 1 ? 1 : 8); ++k) w[k] = NTL == 1 ? 0.0 : d.w[k];
+#pragma unroll
+  for (int r0 = 0; r0 < PER; r0 += G) {
     double v[G][NTL];
 #pragma unroll
     for (int r = 0; r < G; ++r) {
-      const unsigned p = p0 + (r0 + r) * NTHREADS;
+      const unsigned p = p0 + (r0 + r) * LANES;
       if (p < npts) {
         int i, j, k;
         unflatten(d, p, i, j, k);
-        const long long si = (d.soff[0] + i) + (d.soff[1] + j) * d.ssy + (d.soff[2] + k) * d.ssz;
+        const long long si = i + j * d.ssy + k * d.ssz;
 #pragma unroll
-        for (int t = 0; t < NTL; ++t) v[r][t] = __ldg(d.src[t] + si);
+        for (int t = 0; t < NTL; ++t) v[r][t] = __ldg(src[t] + si);
+      }
+    }
+    // the destination index is recomputed rather than held across the loads
+#pragma unroll
+    for (int r = 0; r < G; ++r) {
+      const unsigned p = p0 + (r0 + r) * LANES;
+      if (p < npts) {
+        int i, j, k;
+        unflatten(d, p, i, j, k);
+        dst[i + j * d.dsy + k * d.dsz] = tcombine<FMA, TK, NTL>(w, v[r]);
+      }
+    }
+  }
+}
+
+template <int LANES, class D> __device__ __forceinline__ void restrict_vc_tile(const D &d, int tile, int lid) {
+  constexpr int PER = STILE / LANES, G = stream_group<LANES, 1>();
+  const unsigned npts = (unsigned)d.n[0] * d.n[1] * d.n[2];
+  const unsigned p0 = (unsigned)tile * STILE + lid;
+  const double *s = d.src[0] + (d.soff[0] + d.soff[1] * d.ssy + d.soff[2] * d.ssz);
+  double *dst = d.dst + (d.doff[0] + d.doff[1] * d.dsy + d.doff[2] * d.dsz);
+#pragma unroll
+  for (int r0 = 0; r0 < PER; r0 += G) {
+    double v[G];
+#pragma unroll
+    for (int r = 0; r < G; ++r) {
+      const unsigned p = p0 + (r0 + r) * LANES;
+      if (p < npts) {
+        int i, j, k;
+        unflatten(d, p, i, j, k);
+        v[r] = __ldg(s + 2 * (i + j * d.ssy + k * d.ssz));
       }
     }
 #pragma unroll
     for (int r = 0; r < G; ++r) {
-      const unsigned p = p0 + (r0 + r) * NTHREADS;
+      const unsigned p = p0 + (r0 + r) * LANES;
       if (p < npts) {
         int i, j, k;
         unflatten(d, p, i, j, k);
-        d.dst[(d.doff[0] + i) + (d.doff[1] + j) * d.dsy + (d.doff[2] + k) * d.dsz] =
-            tcombine<FMA, TK, NTL>(d.w, v[r]);
+        dst[i + j * d.dsy + k * d.dsz] = v[r];
       }
     }
   }
 }
 
-template <class D>
-__device__ __forceinline__ void restrict_vc_tile(D &d, int tile) {
+template <int FMA, int LANES, class D>
+__device__ __forceinline__ void restrict_cc_tile(const D &d, int tile, int lid) {
+  constexpr int PER = STILE / LANES;
   const unsigned npts = (unsigned)d.n[0] * d.n[1] * d.n[2];
-  const unsigned p0 = (unsigned)tile * CTILE + threadIdx.x;
-  const double *s = d.src[0];
-  double v[CPT];
-#pragma unroll
-  for (int r = 0; r < CPT; ++r) {
-    const unsigned p = p0 + r * NTHREADS;
-    if (p < npts) {
-      int i, j, k;
-      unflatten(d, p, i, j, k);
-      v[r] = __ldg(s + (d.soff[0] + 2 * i) + (d.soff[1] + 2 * j) * d.ssy + (d.soff[2] + 2 * k) * d.ssz);
-    }
-  }
-#pragma unroll
-  for (int r = 0; r < CPT; ++r) {
-    const unsigned p = p0 + r * NTHREADS;
-    if (p < npts) {
-      int i, j, k;
-      unflatten(d, p, i, j, k);
-      d.dst[(d.doff[0] + i) + (d.doff[1] + j) * d.dsy + (d.doff[2] + k) * d.dsz] = v[r];
-    }
-  }
-}
-
-template <int FMA, class D>
-__device__ __forceinline__ void restrict_cc_tile(D &d, int tile) {
-  const unsigned npts = (unsigned)d.n[0] * d.n[1] * d.n[2];
-  const unsigned p0 = (unsigned)tile * CTILE + threadIdx.x;
+  const unsigned p0 = (unsigned)tile * STILE + lid;
+  const double *s0 = d.src[0] + (d.soff[0] + d.soff[1] * d.ssy + d.soff[2] * d.ssz);
+  double *dst = d.dst + (d.doff[0] + d.doff[1] * d.dsy + d.doff[2] * d.dsz);
+  const long long ssy = d.ssy, ssz = d.ssz;
   const double w = 0.125; // f1*f1*f1 with f1 = f2 = 1/2
 #pragma unroll 2
-  for (int r = 0; r < CPT; ++r) {
-    const unsigned p = p0 + r * NTHREADS;
+  for (int r = 0; r < PER; ++r) {
+    const unsigned p = p0 + r * LANES;
     if (p >= npts) break;
     int i, j, k;
     unflatten(d, p, i, j, k);
-    const double *q = d.src[0] + (d.soff[0] + 2 * i) + (d.soff[1] + 2 * j) * d.ssy +
-                      (d.soff[2] + 2 * k) * d.ssz;
-    const double a0 = __ldg(q), a1 = __ldg(q + 1), a2 = __ldg(q + d.ssy), a3 = __ldg(q + 1 + d.ssy);
-    const double a4 = __ldg(q + d.ssz), a5 = __ldg(q + 1 + d.ssz);
-    const double a6 = __ldg(q + d.ssy + d.ssz), a7 = __ldg(q + 1 + d.ssy + d.ssz);
+    const double *q = s0 + 2 * (i + j * ssy + k * ssz);
+    const double a0 = __ldg(q), a1 = __ldg(q + 1), a2 = __ldg(q + ssy), a3 = __ldg(q + 1 + ssy);
+    const double a4 = __ldg(q + ssz), a5 = __ldg(q + 1 + ssz);
+    const double a6 = __ldg(q + ssy + ssz), a7 = __ldg(q + 1 + ssy + ssz);
     // order of restrict_3d_cc_rf2.cc:253-260
     double res = mul(w, a0);
     res = madd<FMA>(w, a1, res);
@@ -361,7 +382,7 @@ __device__ __forceinline__ void restrict_cc_tile(D &d, int tile) {
     res = madd<FMA>(w, a5, res);
     res = madd<FMA>(w, a6, res);
     res = madd<FMA>(w, a7, res);
-    d.dst[(d.doff[0] + i) + (d.doff[1] + j) * d.dsy + (d.doff[2] + k) * d.dsz] = res;
+    dst[i + j * d.dsy + k * d.dsz] = res;
   }
 }
 

@@ -69,15 +69,17 @@ int klaunch_search_f1(const Desc *d, const long long *prefix, int ndesc, long lo
 int klaunch_spair_f0(const Desc &d, int ntiles, int *status, cudaStream_t s);
 int klaunch_spair_f1(const Desc &d, int ntiles, int *status, cudaStream_t s);
 // TMA prolongation kernels: f<mode>_p0 families 0-4 (VC 1/3/5, CC 0/1),
-// _p1 families 5-9 (CC 2-5, ENO); variant = 4 * family + time variant
-int klaunch_tma_f0_p0(int variant, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
-                      long long ntiles, unsigned long long *counter, int *status, cudaStream_t s);
-int klaunch_tma_f0_p1(int variant, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
-                      long long ntiles, unsigned long long *counter, int *status, cudaStream_t s);
-int klaunch_tma_f1_p0(int variant, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
-                      long long ntiles, unsigned long long *counter, int *status, cudaStream_t s);
-int klaunch_tma_f1_p1(int variant, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
-                      long long ntiles, unsigned long long *counter, int *status, cudaStream_t s);
+// _p1 families 5-9 (CC 2-5, ENO), _c<k> tile configuration TMA_CFGS[k];
+// variant = 4 * family + time variant
+#define CGX_TMA_DECL(F, P, C)                                                                          \
+  int klaunch_tma_f##F##_p##P##_c##C(int variant, const Desc *d, const CUtensorMap *maps,             \
+                                     const int2 *tmap, long long ntiles, unsigned long long *counter, \
+                                     int *status, cudaStream_t s);
+CGX_TMA_DECL(0, 0, 0) CGX_TMA_DECL(0, 0, 1) CGX_TMA_DECL(0, 0, 2)
+CGX_TMA_DECL(0, 1, 0) CGX_TMA_DECL(0, 1, 1) CGX_TMA_DECL(0, 1, 2)
+CGX_TMA_DECL(1, 0, 0) CGX_TMA_DECL(1, 0, 1) CGX_TMA_DECL(1, 0, 2)
+CGX_TMA_DECL(1, 1, 0) CGX_TMA_DECL(1, 1, 1) CGX_TMA_DECL(1, 1, 2)
+#undef CGX_TMA_DECL
 int klaunch_stream_f0(int variant, const Desc *d, const int2 *tmap, long long ntiles,
                       unsigned long long *counter, int *status, cudaStream_t s);
 int klaunch_stream_f1(int variant, const Desc *d, const int2 *tmap, long long ntiles,

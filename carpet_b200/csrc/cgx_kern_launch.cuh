@@ -70,34 +70,45 @@ template <int FMA> int launch_spair_t(const Desc &d, int ntiles, int *status, cu
   return e == cudaSuccess ? CGX_OK : cuda_error(e, "k_spair launch");
 }
 
-template <int FMA, class F, int NTL, int TK>
+template <int FMA, class F, int NTL, int TK, int CFG>
 int launch_tma_v(int variant, const Desc *d_descs, const CUtensorMap *d_maps, const int2 *d_tmap,
                  long long ntiles, unsigned long long *d_counter, int *d_status, cudaStream_t s) {
+  constexpr int NT = TMA_CFGS[CFG].nt;
   static bool attr = false;
-  const size_t smem = sizeof(double) * TSmem<F, NTL>::total + 128; // + alignment slack
+  const size_t smem = sizeof(double) * TSmem<F, NTL, TMA_CFGS[CFG].pyc>::total + 128; // + alignment slack
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_tma_map<FMA, F, NTL, TK>,
+    cudaError_t e = cudaFuncSetAttribute(k_tma_map<FMA, F, NTL, TK, CFG>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute");
     attr = true;
   }
-  int grid = 0;
-  persistent_grid(k_tma_map<FMA, F, NTL, TK>, smem, ntiles, &grid);
-  k_tma_map<FMA, F, NTL, TK><<<grid, NTHREADS, smem, s>>>(d_descs, d_maps, d_tmap, ntiles, d_counter, d_status,
-                                                          variant);
+  int dev = 0, nsm = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tma_map<FMA, F, NTL, TK, CFG>, NT, smem) !=
+          cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  const int grid = (int)std::min<long long>((long long)nsm * per_sm, ntiles);
+  k_tma_map<FMA, F, NTL, TK, CFG><<<grid, NT, smem, s>>>(d_descs, d_maps, d_tmap, ntiles, d_counter, d_status,
+                                                        variant);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? CGX_OK : cuda_error(e, "k_tma_map launch");
 }
 
-// the four time-interpolation variants of one family
-template <int FMA, class F>
+// the four time-interpolation variants of one family, in configuration CFG
+template <int FMA, class F, int CFG>
 int launch_tma_family(int variant, const Desc *d_descs, const CUtensorMap *d_maps, const int2 *d_tmap,
                       long long ntiles, unsigned long long *d_counter, int *d_status, cudaStream_t s) {
   switch (variant % 4) {
-  case 0: return launch_tma_v<FMA, F, 1, T_NONE>(variant, d_descs, d_maps, d_tmap, ntiles, d_counter, d_status, s);
-  case 1: return launch_tma_v<FMA, F, 2, T_LIN>(variant, d_descs, d_maps, d_tmap, ntiles, d_counter, d_status, s);
-  case 2: return launch_tma_v<FMA, F, 3, T_QUAD>(variant, d_descs, d_maps, d_tmap, ntiles, d_counter, d_status, s);
-  default: return launch_tma_v<FMA, F, 3, T_ENO>(variant, d_descs, d_maps, d_tmap, ntiles, d_counter, d_status, s);
+  case 0:
+    return launch_tma_v<FMA, F, 1, T_NONE, CFG>(variant, d_descs, d_maps, d_tmap, ntiles, d_counter, d_status, s);
+  case 1:
+    return launch_tma_v<FMA, F, 2, T_LIN, CFG>(variant, d_descs, d_maps, d_tmap, ntiles, d_counter, d_status, s);
+  case 2:
+    return launch_tma_v<FMA, F, 3, T_QUAD, CFG>(variant, d_descs, d_maps, d_tmap, ntiles, d_counter, d_status, s);
+  default:
+    return launch_tma_v<FMA, F, 3, T_ENO, CFG>(variant, d_descs, d_maps, d_tmap, ntiles, d_counter, d_status, s);
   }
 }
 

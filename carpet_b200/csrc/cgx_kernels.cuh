@@ -39,11 +39,13 @@ __device__ __noinline__ void prolong_entry(const Desc &d, int tile, double *sm) 
 }
 template <int FMA, int NTL, int TK>
 __device__ __noinline__ void copy_entry(const Desc &d, int tile) {
-  copy_tile<FMA, NTL, TK>(d, tile);
+  copy_tile<FMA, NTL, TK, NTHREADS>(d, tile, threadIdx.x);
 }
-static __device__ __noinline__ void restrict_vc_entry(const Desc &d, int tile) { restrict_vc_tile(d, tile); }
+static __device__ __noinline__ void restrict_vc_entry(const Desc &d, int tile) {
+  restrict_vc_tile<NTHREADS>(d, tile, threadIdx.x);
+}
 template <int FMA> __device__ __noinline__ void restrict_cc_entry(const Desc &d, int tile) {
-  restrict_cc_tile<FMA>(d, tile);
+  restrict_cc_tile<FMA, NTHREADS>(d, tile, threadIdx.x);
 }
 
 template <class F, int FMA>
@@ -194,71 +196,81 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 
 
 // Streaming kernels (copy and restrictions): no shared-memory stage, so
-// they run at high occupancy -- many warps keep enough loads in flight.
+// they run at high occupancy -- many warps keep their loads in flight.
 constexpr int STREAM_BLOCKS_PER_SM = 4;
 
-// one streaming variant's tile; V is a StreamVariant
-template <int FMA, int V> __device__ __forceinline__ void stream_tile(const Desc &d, int tile) {
-  if (V == SV_COPY1) copy_tile<FMA, 1, T_NONE>(d, tile);
-  else if (V == SV_COPY2) copy_tile<FMA, 2, T_LIN>(d, tile);
-  else if (V == SV_COPY3Q) copy_tile<FMA, 3, T_QUAD>(d, tile);
-  else if (V == SV_COPY3E) copy_tile<FMA, 3, T_ENO>(d, tile);
-  else if (V == SV_RESTRICT_VC) restrict_vc_tile(d, tile);
-  else restrict_cc_tile<FMA>(d, tile);
+// one streaming variant's tile, run by LANES threads (lid: 0 .. LANES-1);
+// V is a StreamVariant
+template <int FMA, int V, int LANES>
+__device__ __forceinline__ void stream_tile(const Desc &d, int tile, int lid) {
+  if (V == SV_COPY1) copy_tile<FMA, 1, T_NONE, LANES>(d, tile, lid);
+  else if (V == SV_COPY2) copy_tile<FMA, 2, T_LIN, LANES>(d, tile, lid);
+  else if (V == SV_COPY3Q) copy_tile<FMA, 3, T_QUAD, LANES>(d, tile, lid);
+  else if (V == SV_COPY3E) copy_tile<FMA, 3, T_ENO, LANES>(d, tile, lid);
+  else if (V == SV_RESTRICT_VC) restrict_vc_tile<LANES>(d, tile, lid);
+  else restrict_cc_tile<FMA, LANES>(d, tile, lid);
 }
 
-// Per-box form: every variant in one dispatch.  The descriptor parameter
-// is uniform, so its fields are read from the parameter space.
+// Per-box form: a CTA per tile, every variant in one dispatch.  The
+// descriptor parameter is uniform, so its fields are read from the
+// parameter space.
 template <int FMA>
 __global__ void __launch_bounds__(NTHREADS, STREAM_BLOCKS_PER_SM)
     k_spair(const __grid_constant__ Desc d, int *status) {
   __shared__ __align__(16) Desc s_d;
   if (threadIdx.x == 0) s_d = d;
   __syncthreads();
+  const int t = blockIdx.x, l = threadIdx.x;
   switch (stream_variant(s_d)) {
-  case SV_COPY1: stream_tile<FMA, SV_COPY1>(s_d, blockIdx.x); return;
-  case SV_COPY2: stream_tile<FMA, SV_COPY2>(s_d, blockIdx.x); return;
-  case SV_COPY3Q: stream_tile<FMA, SV_COPY3Q>(s_d, blockIdx.x); return;
-  case SV_COPY3E: stream_tile<FMA, SV_COPY3E>(s_d, blockIdx.x); return;
-  case SV_RESTRICT_VC: stream_tile<FMA, SV_RESTRICT_VC>(s_d, blockIdx.x); return;
-  case SV_RESTRICT_CC: stream_tile<FMA, SV_RESTRICT_CC>(s_d, blockIdx.x); return;
+  case SV_COPY1: stream_tile<FMA, SV_COPY1, NTHREADS>(s_d, t, l); return;
+  case SV_COPY2: stream_tile<FMA, SV_COPY2, NTHREADS>(s_d, t, l); return;
+  case SV_COPY3Q: stream_tile<FMA, SV_COPY3Q, NTHREADS>(s_d, t, l); return;
+  case SV_COPY3E: stream_tile<FMA, SV_COPY3E, NTHREADS>(s_d, t, l); return;
+  case SV_RESTRICT_VC: stream_tile<FMA, SV_RESTRICT_VC, NTHREADS>(s_d, t, l); return;
+  case SV_RESTRICT_CC: stream_tile<FMA, SV_RESTRICT_CC, NTHREADS>(s_d, t, l); return;
   }
   if (threadIdx.x == 0) report(status, CGX_EDEVICE);
 }
 
 // Persistent form: one kernel per variant over that variant's segment of
-// the tile map.  The descriptor fields are shared-memory reads that the
-// compiler keeps in registers; one variant per kernel keeps that within the
-// register budget of STREAM_BLOCKS_PER_SM CTAs per SM.
+// the tile map, a CTA per tile.  One barrier per tile: thread 0 claims the
+// tile after next (a three-slot ring of claims) and the CTA stages the next
+// tile's descriptor into the second of two shared buffers while the current
+// tile runs.
 template <int FMA, int V>
 __global__ void __launch_bounds__(NTHREADS, STREAM_BLOCKS_PER_SM)
     k_stream_map(const Desc *__restrict__ descs, const int2 *__restrict__ tmap, long long ntiles,
                  unsigned long long *counter, int *status) {
-  __shared__ long long s_t, s_next;
-  __shared__ int2 s_m;
-  __shared__ __align__(16) Desc s_d;
-  if (threadIdx.x == 0) {
+  __shared__ __align__(16) Desc s_d[2];
+  __shared__ long long s_t[3];
+  __shared__ int2 s_m[3];
+  const int tid = threadIdx.x;
+  constexpr int DW = sizeof(Desc) / 8;
+  auto claim = [&](int slot) {
     const long long t = (long long)atomicAdd(counter, 1ULL);
-    s_t = t;
-    s_m = t < ntiles ? tmap[t] : make_int2(0, 0);
+    s_t[slot] = t;
+    s_m[slot] = t < ntiles ? tmap[t] : make_int2(0, 0);
+  };
+  auto stage = [&](int buf, int slot) {
+    if (tid < DW && s_t[slot] < ntiles)
+      reinterpret_cast<unsigned long long *>(&s_d[buf])[tid] =
+          __ldg(reinterpret_cast<const unsigned long long *>(descs + s_m[slot].x) + tid);
+  };
+  if (tid == 0) {
+    claim(0);
+    claim(1);
   }
   __syncthreads();
-  for (;;) {
-    if (s_t >= ntiles) break;
-    const int2 m = s_m;
-    if (threadIdx.x < sizeof(Desc) / 8)
-      reinterpret_cast<unsigned long long *>(&s_d)[threadIdx.x] =
-          __ldg(reinterpret_cast<const unsigned long long *>(descs + m.x) + threadIdx.x);
-    if (threadIdx.x == 0) s_next = (long long)atomicAdd(counter, 1ULL);
-    __syncthreads();
-    if (stream_variant(s_d) == V) stream_tile<FMA, V>(s_d, m.y);
-    else if (threadIdx.x == 0) report(status, CGX_EDEVICE);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const long long tn = s_next;
-      s_t = tn;
-      s_m = tn < ntiles ? tmap[tn] : make_int2(0, 0);
-    }
+  stage(0, 0);
+  __syncthreads();
+  for (int i = 0;; ++i) {
+    const int slot = i % 3, buf = i & 1;
+    if (s_t[slot] >= ntiles) break;
+    const int tile = s_m[slot].y;
+    if (tid == 0) claim((i + 2) % 3);
+    stage(buf ^ 1, (i + 1) % 3);
+    if (stream_variant(s_d[buf]) == V) stream_tile<FMA, V, NTHREADS>(s_d[buf], tile, tid);
+    else if (tid == 0) report(status, CGX_EDEVICE);
     __syncthreads();
   }
 }
@@ -268,8 +280,8 @@ __global__ void __launch_bounds__(NTHREADS, STREAM_BLOCKS_PER_SM)
 // interpolation), so that each gets its own register allocation; maps[3 * i
 // + t] is the tensor map of descriptor i's timelevel t.  The claim loop is
 // that of k_stream_map.
-template <int FMA, class F, int NTL, int TK>
-__global__ void __launch_bounds__(NTHREADS, 2)
+template <int FMA, class F, int NTL, int TK, int CFG>
+__global__ void __launch_bounds__(TMA_CFGS[CFG].nt, 512 / TMA_CFGS[CFG].nt)
     k_tma_map(const Desc *__restrict__ descs, const CUtensorMap *__restrict__ maps,
               const int2 *__restrict__ tmap, long long ntiles, unsigned long long *counter, int *status,
               int variant) {
@@ -302,7 +314,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     if (threadIdx.x == 0) s_next = (long long)atomicAdd(counter, 1ULL);
     __syncthreads();
     if (tma_variant(s_d) == variant) {
-      if (!prolong_tile_tma<F, FMA, NTL, TK>(s_d, maps + 3 * (size_t)m.x, m.y, sm, ring, status)) return;
+      if (!prolong_tile_tma<F, FMA, NTL, TK, CFG>(s_d, maps + 3 * (size_t)m.x, m.y, sm, ring, status)) return;
     } else if (threadIdx.x == 0) {
       report(status, CGX_EDEVICE);
     }

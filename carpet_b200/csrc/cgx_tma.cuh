@@ -25,12 +25,21 @@
 
 namespace cgx {
 
-template <class F> struct TGeom {
+// Tile configurations the autotuner chooses between: threads per CTA, coarse
+// y rows per tile (threads / 16: one thread per fine x and coarse row) and
+// fine z points per tile.  Configuration 0 is the default.
+struct TmaCfg {
+  int nt, pyc, pz;
+};
+constexpr TmaCfg TMA_CFGS[] = {{256, 16, 64}, {128, 8, 64}, {128, 8, 32}};
+constexpr int TMA_NCFG = 3;
+
+template <class F, int PYC = PTYCMAX> struct TGeom {
   static constexpr int W = F::HI - F::LO;
   // box: up to (PTXMAX + 2) / 2 coarse bases + the window + one point of
   // even-alignment shift, rounded up to even; by = ptyc + W rows
   static constexpr int BXMAX = ((PTXMAX + 2) / 2 + W + 2) & ~1;
-  static constexpr int BYMAX = PTYCMAX + W;
+  static constexpr int BYMAX = PYC + W;
   static constexpr int TLS = (BXMAX * BYMAX + 15) / 16 * 16; // doubles per (slot, timelevel)
   static constexpr int CY = BYMAX;                            // x-pass rows per timelevel
   // x-pass row pitch: two fine points per coarse base; the y pass's lane
@@ -41,8 +50,8 @@ template <class F> struct TGeom {
 };
 constexpr int TMA_PD = 3;          // planes in flight ahead of the x pass
 constexpr int TMA_NB = TMA_PD + 2; // ring slots
-template <class F, int NTL> struct TSmem {
-  using G = TGeom<F>;
+template <class F, int NTL, int PYC = PTYCMAX> struct TSmem {
+  using G = TGeom<F, PYC>;
   static constexpr int coarse = TMA_NB * NTL * G::TLS;
   static constexpr int xbuf = (NTL * G::CY + 1) * G::XR; // + one row for masked x items
   static constexpr int total = coarse + 2 * xbuf;        // doubles
@@ -117,11 +126,12 @@ struct TmaRing {
 
 // One prolongation tile.  Returns false when a wait gave up (the CTA then
 // stops; the status word holds CGX_EDEVICE).
-template <class F, int FMA, int NTL, int TK>
+template <class F, int FMA, int NTL, int TK, int CFG>
 __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ maps, int tile, double *sm,
                                  TmaRing &ring, int *status) {
-  using G = TGeom<F>;
-  using S = TSmem<F, NTL>;
+  constexpr int NT = TMA_CFGS[CFG].nt, PYC = TMA_CFGS[CFG].pyc, PZ = TMA_CFGS[CFG].pz;
+  using G = TGeom<F, PYC>;
+  using S = TSmem<F, NTL, PYC>;
   constexpr int LO = F::LO, HI = F::HI, Q = G::Q, NB = TMA_NB, PD = TMA_PD;
   const int tid = threadIdx.x;
   const int ptx = d.ptx, ptyc = d.ptyc, pty = 2 * ptyc - 1;
@@ -130,8 +140,8 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
 
   const int tx = tile % d.tiles[0], rr = tile / d.tiles[0];
   const int ty = rr % d.tiles[1], tz = rr / d.tiles[1];
-  const int fx0 = tx * ptx, fy0 = ty * pty, fz0 = tz * PTZ;
-  const int nfx = min(ptx, d.n[0] - fx0), nfy = min(pty, d.n[1] - fy0), nfz = min(PTZ, d.n[2] - fz0);
+  const int fx0 = tx * ptx, fy0 = ty * pty, fz0 = tz * PZ;
+  const int nfx = min(ptx, d.n[0] - fx0), nfy = min(pty, d.n[1] - fy0), nfz = min(PZ, d.n[2] - fz0);
   const int sx0 = d.soff[0] + fx0, sy0 = d.soff[1] + fy0, sz0 = d.soff[2] + fz0;
   const int c_first = sx0 >> 1, c_last = (sx0 + nfx - 1) >> 1;
   const int cx0 = c_first + LO;
@@ -159,12 +169,12 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
   };
 
   // --- x items: (timelevel, row, base) spread over the CTA
-  constexpr int IT = (NTL * G::CY * ((PTXMAX + 2) / 2) + NTHREADS - 1) / NTHREADS; // nbx <= 9
+  constexpr int IT = (NTL * G::CY * ((PTXMAX + 2) / 2) + NT - 1) / NT; // nbx <= 9
   const int per_t = ncy * nbx, count = NTL * per_t;
   int xsrc[IT], xdst[IT];
 #pragma unroll
   for (int k = 0; k < IT; ++k) {
-    const int it = tid + k * NTHREADS;
+    const int it = tid + k * NT;
     if (it < count) {
       const int t = it / per_t, rem = it - t * per_t;
       const int r = rem / nbx, b = rem - r * nbx;
@@ -179,7 +189,7 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
     const double *__restrict__ cs = coarse + slot * NTL * G::TLS - LO;
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
-      if (k * NTHREADS < count) { // uniform
+      if (k * NT < count) { // uniform
         const double *row = cs + xsrc[k];
         auto get = [&](int m) { return row[m]; };
         const double xe = F::template first<FMA>(0, get);
@@ -190,7 +200,7 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
   };
 
   // --- y/z owner: thread = (fine x, coarse y row) = (tid % 16, tid / 16)
-  static_assert(PTXMAX == 16 && NTHREADS == 16 * PTYCMAX, "y/z thread layout");
+  static_assert(PTXMAX == 16 && NT == 16 * PYC, "y/z thread layout");
   const int my_fx = tid & 15, my_cyr = tid >> 4;
   const bool tact = my_fx < ptx && my_cyr < ptyc;
   const bool wact = 2 * (tid >> 5) < ptyc; // warp holds an owner

@@ -154,7 +154,8 @@ def nested(nlevels: int, npoints, parts=(2, 2, 2), ghost=3, buffer=9, order=5,
            origin=(0, 0, 0)) -> Hierarchy:
     """``nlevels`` vertex-centred levels of ``npoints`` points per axis each
     (an int or one per axis, each 1 mod 4), each level covering the central
-    half of the next coarser one."""
+    half of the next coarser one; ``parts`` splits every level into
+    components (one (px, py, pz) for all levels, or a list of one per level)."""
     n = (npoints,) * 3 if isinstance(npoints, int) else tuple(npoints)
     assert all((m - 1) % 4 == 0 for m in n)
     st0 = 2 ** (nlevels - 1)
@@ -163,7 +164,8 @@ def nested(nlevels: int, npoints, parts=(2, 2, 2), ghost=3, buffer=9, order=5,
     for l in range(nlevels):
         st = st0 >> l
         box = mkbox(lo, [lo[d] + (n[d] - 1) * st for d in range(3)], (st,) * 3)
-        levels.append(build_level(box, parts, ghost))
+        lp = parts[l] if isinstance(parts[0], (tuple, list)) else parts
+        levels.append(build_level(box, lp, ghost))
         # next level: the central half, (n-1)/4 coarse points in
         lo = [lo[d] + ((n[d] - 1) // 4) * st for d in range(3)]
     h = Hierarchy(levels, ghost, buffer, order)

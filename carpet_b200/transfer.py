@@ -148,6 +148,19 @@ class Batch:
         check(lib.cgx_batch_stats(self.h, *[C.byref(x) for x in v]))
         return dict(pairs=v[0].value, tiles=v[1].value, points=v[2].value, bytes=v[3].value)
 
+    def autotune(self, reps: int = 3, stream=None):
+        """pick the fastest tile configuration of every prolongation variant
+        in the batch (runs the batch; leaves it uploaded); returns
+        {variant: configuration}"""
+        out = (C.c_int * 40)()
+        check(lib.cgx_batch_autotune(self.h, reps, _stream(stream), out))
+        return {v: out[v] for v in range(40) if out[v] >= 0}
+
+    def set_config(self, config: int, variant: int = -1):
+        """pin the tile configuration of one prolongation variant (all: -1);
+        takes effect at the next upload()"""
+        check(lib.cgx_batch_set_config(self.h, variant, config))
+
     def kernels(self) -> int:
         """kernels one launch() issues for the current upload"""
         n = C.c_int()

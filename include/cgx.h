@@ -134,6 +134,19 @@ int cgx_batch_launch(cgx_batch *b, void *stream);
 /* kernels one cgx_batch_launch issues for the current upload (no
  * counterpart in the reference: a measurement aid) */
 int cgx_batch_kernels(const cgx_batch *b, int *nkernels);
+/* Tile-shape autotuner (no counterpart in the reference): uploads the
+ * batch, times every prolongation variant it holds in each of the library's
+ * tile configurations (reps launches each, on the caller's arrays -- the
+ * results written are those of a normal launch) and keeps the fastest.
+ * chosen (nullable) receives CGX_TMA_VARIANTS entries: the configuration
+ * index per variant, -1 where the batch has none.  Synchronises stream. */
+#define CGX_TMA_VARIANTS 40
+#define CGX_TMA_CONFIGS 3
+int cgx_batch_autotune(cgx_batch *b, int reps, void *stream, int *chosen);
+/* pin the tile configuration (0 .. CGX_TMA_CONFIGS-1) of one prolongation
+ * variant, or of all with variant = -1 (e.g. a saved autotune result);
+ * takes effect at the next cgx_batch_upload */
+int cgx_batch_set_config(cgx_batch *b, int variant, int config);
 /* plain per-box launches of the same descriptors (one kernel per pair) */
 int cgx_batch_launch_per_box(cgx_batch *b, void *stream);
 /* device status word of the last launches: 0 or a CGX_E* code */

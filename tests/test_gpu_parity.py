@@ -200,10 +200,22 @@ def test_batched_mixed_pairs_match_per_box_and_oracle(cgx, port, fma):
     st = b.stats()
     assert st["pairs"] == 60 and st["tiles"] > 60
     b.upload()
-    for mode in ("batch", "per_box", "graph"):
+    modes = ["batch", "per_box", "graph"] + [f"config{c}" for c in range(3)] + ["autotuned"]
+    for mode in modes:
         for dst, _, _, init in items:
             dst.tensor.copy_(torch.from_numpy(init))
-        if mode == "batch":
+        if mode.startswith("config"):
+            # every prolongation variant pinned to one tile configuration
+            b.set_config(int(mode[6:]))
+            b.upload()
+            b.launch()
+        elif mode == "autotuned":
+            chosen = b.autotune(reps=2)
+            assert chosen and all(0 <= c < 3 for c in chosen.values())
+            for dst, _, _, init in items:  # autotuning ran the batch: start over
+                dst.tensor.copy_(torch.from_numpy(init))
+            b.launch()
+        elif mode == "batch":
             b.launch()
         elif mode == "per_box":
             b.launch_per_box()
