@@ -20,6 +20,8 @@ roofline     the dominant kernel (the phase kind with the largest share of
              the step): its algorithmic bytes per launch / its CUDA-event time
 cpu_baseline CarpetLib's own operators (compiled from the reference) on the
              host cores, a bounded sample of the same step
+served       the served ensemble (64 hierarchies, Poisson request stream)
+batched_uneven  256 uneven mixed box-pairs, autotuned + graph vs per box
 
 --impl reference: only the CPU reference arm (rank 0).
 """
@@ -68,6 +70,7 @@ def parse():
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--serve-seconds", type=float, default=1.0)
     p.add_argument("--no-tune", action="store_true", help="default tile configurations")
+    p.add_argument("--no-uneven", action="store_true", help="skip the batched uneven section")
     return p.parse_args()
 
 
@@ -347,6 +350,53 @@ def served(seconds: float):
     return out
 
 
+# ----------------------------------------------------------------- uneven
+def uneven(steps: int, warmup: int, fp: str):
+    """Batched uneven configuration: 256 box-pairs, fine extents U{16..96}
+    per axis, operators 40/20/20/20 vc Lagrange o5 / vc ENO o3 / cc Lagrange
+    o3 / cc averaging; autotuned tiles, one graph replay per step, against the
+    plain per-box launches of the same descriptors."""
+    import torch
+    import carpet_b200 as cb
+    from carpet_b200.uneven import uneven_batch, uneven_pairs, uneven_specs
+    cb.set_fp_mode(fp == "fma")
+    pairs = uneven_pairs(uneven_specs(seed=3, npairs=256, ext=(16, 96)), seed=4)
+    b = uneven_batch(pairs)
+    st = b.stats()
+    tuned = b.autotune(reps=3)
+    s = torch.cuda.Stream()
+    g = cb.Graph()
+    with g.capture(s):
+        b.launch(s)
+
+    def timed(fn, k):
+        for _ in range(warmup):
+            fn()
+        s.synchronize()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        for _ in range(k):
+            fn()
+        e.record(s)
+        s.synchronize()
+        return a.elapsed_time(e) / k
+
+    ms = timed(lambda: g.launch(s), steps)
+    batched = [p.dst.tensor.clone() for p in pairs]
+    pms = timed(lambda: b.launch_per_box(s), max(1, steps // 2))
+    same = all(torch.equal(x.view(torch.int64), p.dst.tensor.view(torch.int64))
+               for x, p in zip(batched, pairs))
+    b.check(s)
+    return {"workload": "256 box-pairs, fine extents U{16..96}^3, 40% vc Lagrange o5, 20% vc ENO o3, "
+                        "20% cc Lagrange o3, 20% cc averaging; autotuned, graph replay",
+            "pairs": st["pairs"], "fine_points": st["points"], "bytes": st["bytes"],
+            "ms": round(ms, 4), "gbs": round(st["bytes"] / (ms * 1e-3) / 1e9, 1),
+            "fine_points_per_s": round(st["points"] / (ms * 1e-3), 1),
+            "plain_ms": round(pms, 4), "plain_gbs": round(st["bytes"] / (pms * 1e-3) / 1e9, 1),
+            "batched_vs_plain": round(pms / ms, 2), "identical_to_plain": bool(same),
+            "tile_configs": sorted(set(tuned.values()))}
+
+
 # ----------------------------------------------------------------- main
 def main():
     args = parse()
@@ -541,6 +591,10 @@ def main():
     if rank == 0 and not args.no_serve:
         serve = served(args.serve_seconds)
 
+    batched_uneven = None
+    if rank == 0 and not args.no_uneven:
+        batched_uneven = uneven(max(args.steps, 3), args.warmup, args.fp)
+
     # DRAM bytes per launch of the dominant kernel: the ratio of DRAM bytes
     # to algorithmic bytes that ncu measured on a smaller capture of the same
     # kernel (profiles/traffic.json), scaled to this launch
@@ -577,6 +631,7 @@ def main():
                          else "fallback 6650 GB/s"},
             "phases": phases,
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(), "served": serve,
+            "batched_uneven": batched_uneven,
         }
         print(json.dumps(out))
     for g in graphs:
