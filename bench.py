@@ -22,6 +22,8 @@ cpu_baseline CarpetLib's own operators (compiled from the reference) on the
              host cores, a bounded sample of the same step
 served       the served ensemble (64 hierarchies, Poisson request stream)
 batched_uneven  256 uneven mixed box-pairs, autotuned + graph vs per box
+moving_boxes (--moving) the 8-level moving-box hierarchy: a coarse step and a
+             regrid (host schedule + batched graph fill)
 
 --impl reference: only the CPU reference arm (rank 0).
 """
@@ -71,6 +73,8 @@ def parse():
     p.add_argument("--serve-seconds", type=float, default=1.0)
     p.add_argument("--no-tune", action="store_true", help="default tile configurations")
     p.add_argument("--no-uneven", action="store_true", help="skip the batched uneven section")
+    p.add_argument("--moving", action="store_true",
+                   help="add the moving-box section (~80 GB on the device, minutes)")
     return p.parse_args()
 
 
@@ -397,6 +401,85 @@ def uneven(steps: int, warmup: int, fp: str):
             "tile_configs": sorted(set(tuned.values()))}
 
 
+# ----------------------------------------------------------------- moving
+def moving(ngf: int, fp: str, steps: int):
+    """Moving-box configuration: 8 vertex-centred levels (a 257^3 coarse level
+    in 16 components; 7 refined levels of two 161^3 boxes, 8 components each,
+    around two centres orbiting at 0.3 L, one revolution per 256 coarse
+    steps), ngf grid functions x 3 timelevels.  Times one coarse
+    Berger-Oliger step (order-5 prolongation with quadratic time
+    interpolation, injection, sync; graph replay) and one regrid after 8
+    coarse steps: the host schedule recompute (hierarchy, old-to-new pairs,
+    descriptors) and the batched, graph-captured fill of every refined level
+    and timelevel on the GPU."""
+    import time
+    import torch
+    import carpet_b200 as cb
+    from carpet_b200.amr import BergerOliger, Storage
+    from carpet_b200.moving import MovingSpec, Regrid, build
+    cb.set_fp_mode(fp == "fma")
+    spec = MovingSpec()
+    h0 = build(spec, 0)
+    st = Storage(h0, ngf, 3)
+    fill_storage(st, h0, seed=5)
+    s = torch.cuda.Stream()
+    # one coarse step
+    bo = BergerOliger(h0, st, order_space=5, order_time=2)
+    keys = bo.step_phases()
+    tuned = bo.autotune(keys, reps=1)
+    g = cb.Graph()
+    with g.capture(s):
+        bo.run(keys, s)
+    g.launch(s)
+    s.synchronize()
+    a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    for _ in range(steps):
+        g.launch(s)
+    e.record(s)
+    s.synchronize()
+    step_ms = a.elapsed_time(e) / steps
+    sst = bo.stats(keys)
+    for b in bo.batches.values():
+        b.check(s)
+    del g
+    # one regrid: host schedule, then the device fill
+    t0 = time.perf_counter()
+    h1 = build(spec, spec.regrid_every)
+    tb = time.perf_counter()
+    new = Storage(h1, ngf, 3, share=st, shared_levels=(0,))
+    t1 = time.perf_counter()
+    rg = Regrid(h0, h1, ngf, 3, lambda l, tl: st.data[l][bo.pool_index(bo.rot[l], tl)],
+                lambda l, tl: (st.data[0][bo.pool_index(bo.rot[0], tl)] if l == 0 else new.data[l][tl]))
+    rg.upload()
+    t2 = time.perf_counter()
+    rst = rg.stats()
+    gr = rg.graph(s)
+    gr.launch(s)
+    s.synchronize()
+    a.record(s)
+    gr.launch(s)
+    e.record(s)
+    s.synchronize()
+    fill_ms = a.elapsed_time(e)
+    for b in rg.batches:
+        b.check(s)
+    out = {"workload": "8 vc levels: 257^3 coarse (16 comps) + 7 levels of two 161^3 boxes (16 comps) "
+                       f"orbiting at 0.3 L; {ngf} GFs x 3 TLs, order-5 + quadratic time interpolation; "
+                       "regrid after 8 coarse steps",
+           "resident_gb": round(st.nbytes() / 1e9, 1),
+           "step_ms": round(step_ms, 2), "step_gbs": round(sst["bytes"] / (step_ms * 1e-3) / 1e9, 1),
+           "step_phases": len(keys), "step_kernels": sst["kernels"],
+           "regrid_host_ms": round((tb - t0 + t2 - t1) * 1e3, 1),
+           "regrid_alloc_ms": round((t1 - tb) * 1e3, 1),
+           "regrid_fill_ms": round(fill_ms, 3),
+           "regrid_fill_gbs": round(rst["bytes"] / (fill_ms * 1e-3) / 1e9, 1),
+           "regrid_pairs": rst["pairs"], "regrid_fine_points": rst["points"],
+           "tile_configs": sorted({c for v in tuned.values() for c in v.values()})}
+    del gr
+    return out
+
+
 # ----------------------------------------------------------------- main
 def main():
     args = parse()
@@ -595,6 +678,10 @@ def main():
     if rank == 0 and not args.no_uneven:
         batched_uneven = uneven(max(args.steps, 3), args.warmup, args.fp)
 
+    moving_boxes = None
+    if rank == 0 and args.moving:
+        moving_boxes = moving(args.ngf, args.fp, 2)
+
     # DRAM bytes per launch of the dominant kernel: the ratio of DRAM bytes
     # to algorithmic bytes that ncu measured on a smaller capture of the same
     # kernel (profiles/traffic.json), scaled to this launch
@@ -631,7 +718,7 @@ def main():
                          else "fallback 6650 GB/s"},
             "phases": phases,
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(), "served": serve,
-            "batched_uneven": batched_uneven,
+            "batched_uneven": batched_uneven, "moving_boxes": moving_boxes,
         }
         print(json.dumps(out))
     for g in graphs:

@@ -24,7 +24,7 @@ the persistent kernel; a whole coarse step can be captured as a CUDA graph.
 from __future__ import annotations
 
 from dataclasses import dataclass
-from typing import Dict, List, Tuple
+from typing import Dict, List, Optional, Tuple
 
 import numpy as np
 import torch
@@ -55,11 +55,19 @@ def storage_bytes(h: Hierarchy, ngf: int, ntl: int) -> int:
 class Storage:
     """[level][tl] -> one pool; data[level][tl][gf][comp] -> Data views"""
 
-    def __init__(self, h: Hierarchy, ngf: int, ntl: int, device="cuda"):
+    def __init__(self, h: Hierarchy, ngf: int, ntl: int, device="cuda",
+                 share: Optional["Storage"] = None, shared_levels=()):
+        """``share`` / ``shared_levels``: levels whose pools are taken from
+        another storage of a hierarchy with the same components there (the
+        unchanged coarse levels of a regrid) instead of allocated"""
         self.h, self.ngf, self.ntl = h, ngf, ntl
         self.pools: List[List[torch.Tensor]] = []
         self.data: List[List[List[List[Data]]]] = []
-        for lev in h.levels:
+        for l, lev in enumerate(h.levels):
+            if share is not None and l in shared_levels:
+                self.pools.append(share.pools[l])
+                self.data.append(share.data[l])
+                continue
             shapes = [_padded(c.exterior) for c in lev.comps]
             # 256-byte aligned offsets for every component array
             offs, n = [], 0
