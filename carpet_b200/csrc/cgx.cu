@@ -501,11 +501,12 @@ int launch_pair(const Desc &d, int ntiles, int fp, int *status, cudaStream_t s) 
 // the TMA kernels' launchers, [fused][family part][configuration]
 using TmaLaunch = int (*)(int, const Desc *, const CUtensorMap *, const int2 *, long long,
                           unsigned long long *, int *, cudaStream_t);
-const TmaLaunch kTmaLaunch[2][2][TMA_NCFG] = {
-    {{klaunch_tma_f0_p0_c0, klaunch_tma_f0_p0_c1, klaunch_tma_f0_p0_c2},
-     {klaunch_tma_f0_p1_c0, klaunch_tma_f0_p1_c1, klaunch_tma_f0_p1_c2}},
-    {{klaunch_tma_f1_p0_c0, klaunch_tma_f1_p0_c1, klaunch_tma_f1_p0_c2},
-     {klaunch_tma_f1_p1_c0, klaunch_tma_f1_p1_c1, klaunch_tma_f1_p1_c2}}};
+#define CGX_TMA_ROW(F, P)                                                                      \
+  {klaunch_tma_f##F##_p##P##_c0, klaunch_tma_f##F##_p##P##_c1, klaunch_tma_f##F##_p##P##_c2, \
+   klaunch_tma_f##F##_p##P##_c3, klaunch_tma_f##F##_p##P##_c4}
+const TmaLaunch kTmaLaunch[2][2][TMA_NCFG] = {{CGX_TMA_ROW(0, 0), CGX_TMA_ROW(0, 1)},
+                                              {CGX_TMA_ROW(1, 0), CGX_TMA_ROW(1, 1)}};
+#undef CGX_TMA_ROW
 
 int launch_map(int fp, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
                const long long seg[NSEG + 1], const int *cfg, unsigned long long *counter, int *status,

@@ -75,10 +75,10 @@ int klaunch_spair_f1(const Desc &d, int ntiles, int *status, cudaStream_t s);
   int klaunch_tma_f##F##_p##P##_c##C(int variant, const Desc *d, const CUtensorMap *maps,             \
                                      const int2 *tmap, long long ntiles, unsigned long long *counter, \
                                      int *status, cudaStream_t s);
-CGX_TMA_DECL(0, 0, 0) CGX_TMA_DECL(0, 0, 1) CGX_TMA_DECL(0, 0, 2)
-CGX_TMA_DECL(0, 1, 0) CGX_TMA_DECL(0, 1, 1) CGX_TMA_DECL(0, 1, 2)
-CGX_TMA_DECL(1, 0, 0) CGX_TMA_DECL(1, 0, 1) CGX_TMA_DECL(1, 0, 2)
-CGX_TMA_DECL(1, 1, 0) CGX_TMA_DECL(1, 1, 1) CGX_TMA_DECL(1, 1, 2)
+#define CGX_TMA_DECL5(F, P) \
+  CGX_TMA_DECL(F, P, 0) CGX_TMA_DECL(F, P, 1) CGX_TMA_DECL(F, P, 2) CGX_TMA_DECL(F, P, 3) CGX_TMA_DECL(F, P, 4)
+CGX_TMA_DECL5(0, 0) CGX_TMA_DECL5(0, 1) CGX_TMA_DECL5(1, 0) CGX_TMA_DECL5(1, 1)
+#undef CGX_TMA_DECL5
 #undef CGX_TMA_DECL
 int klaunch_stream_f0(int variant, const Desc *d, const int2 *tmap, long long ntiles,
                       unsigned long long *counter, int *status, cudaStream_t s);

@@ -75,7 +75,8 @@ int launch_tma_v(int variant, const Desc *d_descs, const CUtensorMap *d_maps, co
                  long long ntiles, unsigned long long *d_counter, int *d_status, cudaStream_t s) {
   constexpr int NT = TMA_CFGS[CFG].nt;
   static bool attr = false;
-  const size_t smem = sizeof(double) * TSmem<F, NTL, TMA_CFGS[CFG].pyc>::total + 128; // + alignment slack
+  const size_t smem =
+      sizeof(double) * TSmem<F, NTL, TMA_CFGS[CFG].pyc, TMA_CFGS[CFG].pd + 2>::total + 128; // + alignment slack
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(k_tma_map<FMA, F, NTL, TK, CFG>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

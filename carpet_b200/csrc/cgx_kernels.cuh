@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(NTHREADS, STREAM_BLOCKS_PER_SM)
 // + t] is the tensor map of descriptor i's timelevel t.  The claim loop is
 // that of k_stream_map.
 template <int FMA, class F, int NTL, int TK, int CFG>
-__global__ void __launch_bounds__(TMA_CFGS[CFG].nt, 512 / TMA_CFGS[CFG].nt)
+__global__ void __launch_bounds__(TMA_CFGS[CFG].nt, TMA_CFGS[CFG].mb)
     k_tma_map(const Desc *__restrict__ descs, const CUtensorMap *__restrict__ maps,
               const int2 *__restrict__ tmap, long long ntiles, unsigned long long *counter, int *status,
               int variant) {
@@ -293,10 +293,10 @@ __global__ void __launch_bounds__(TMA_CFGS[CFG].nt, 512 / TMA_CFGS[CFG].nt)
   __shared__ long long s_t, s_next;
   __shared__ int2 s_m;
   __shared__ __align__(16) Desc s_d;
-  __shared__ __align__(8) uint64_t s_bars[TMA_NB];
+  __shared__ __align__(8) uint64_t s_bars[TMA_NB_MAX];
   __shared__ int s_abort;
   if (threadIdx.x == 0) {
-    for (int i = 0; i < TMA_NB; ++i) mbar_init(&s_bars[i], 1);
+    for (int i = 0; i < TMA_NB_MAX; ++i) mbar_init(&s_bars[i], 1);
     mbar_fence_init();
     s_abort = 0;
     const long long t = (long long)atomicAdd(counter, 1ULL);

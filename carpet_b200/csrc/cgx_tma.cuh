@@ -26,13 +26,16 @@
 namespace cgx {
 
 // Tile configurations the autotuner chooses between: threads per CTA, coarse
-// y rows per tile (threads / 16: one thread per fine x and coarse row) and
-// fine z points per tile.  Configuration 0 is the default.
+// y rows per tile (threads / 16: one thread per fine x and coarse row), fine
+// z points per tile, CTAs per SM the register allocation must allow, and
+// planes staged ahead of the x pass.  Configuration 0 is the default.
 struct TmaCfg {
-  int nt, pyc, pz;
+  int nt, pyc, pz, mb, pd;
 };
-constexpr TmaCfg TMA_CFGS[] = {{256, 16, 64}, {128, 8, 64}, {128, 8, 32}};
-constexpr int TMA_NCFG = 3;
+constexpr TmaCfg TMA_CFGS[] = {
+    {256, 16, 64, 2, 3}, {128, 8, 64, 4, 3}, {128, 8, 32, 4, 3}, {128, 8, 64, 5, 2}, {128, 8, 32, 6, 2}};
+constexpr int TMA_NCFG = 5;
+constexpr int TMA_NB_MAX = 5; // ring slots, at most (pd + 2)
 
 template <class F, int PYC = PTYCMAX> struct TGeom {
   static constexpr int W = F::HI - F::LO;
@@ -48,11 +51,9 @@ template <class F, int PYC = PTYCMAX> struct TGeom {
   static constexpr int XR = 2 * PTXMAX;
   static constexpr int Q = W + 1;
 };
-constexpr int TMA_PD = 3;          // planes in flight ahead of the x pass
-constexpr int TMA_NB = TMA_PD + 2; // ring slots
-template <class F, int NTL, int PYC = PTYCMAX> struct TSmem {
+template <class F, int NTL, int PYC = PTYCMAX, int NB = 5> struct TSmem {
   using G = TGeom<F, PYC>;
-  static constexpr int coarse = TMA_NB * NTL * G::TLS;
+  static constexpr int coarse = NB * NTL * G::TLS;
   static constexpr int xbuf = (NTL * G::CY + 1) * G::XR; // + one row for masked x items
   static constexpr int total = coarse + 2 * xbuf;        // doubles
 };
@@ -119,7 +120,7 @@ __device__ __forceinline__ void tma_load_3d(double *dst, const CUtensorMap *map,
 // whose phase g / NB completes when it lands), and a flag that a wait ran
 // out.  Everything here is uniform over the CTA.
 struct TmaRing {
-  uint64_t *bars; // TMA_NB mbarriers, arrival count 1
+  uint64_t *bars; // pd + 2 mbarriers, arrival count 1
   int *abort;     // shared flag, set when a wait gave up
   unsigned g;     // planes staged by this CTA before the current tile
 };
@@ -130,9 +131,10 @@ template <class F, int FMA, int NTL, int TK, int CFG>
 __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ maps, int tile, double *sm,
                                  TmaRing &ring, int *status) {
   constexpr int NT = TMA_CFGS[CFG].nt, PYC = TMA_CFGS[CFG].pyc, PZ = TMA_CFGS[CFG].pz;
+  constexpr int PD = TMA_CFGS[CFG].pd, NB = PD + 2;
   using G = TGeom<F, PYC>;
-  using S = TSmem<F, NTL, PYC>;
-  constexpr int LO = F::LO, HI = F::HI, Q = G::Q, NB = TMA_NB, PD = TMA_PD;
+  using S = TSmem<F, NTL, PYC, NB>;
+  constexpr int LO = F::LO, HI = F::HI, Q = G::Q;
   const int tid = threadIdx.x;
   const int ptx = d.ptx, ptyc = d.ptyc, pty = 2 * ptyc - 1;
   const int BX = d.bx, BY = d.by;

@@ -141,7 +141,7 @@ int cgx_batch_kernels(const cgx_batch *b, int *nkernels);
  * chosen (nullable) receives CGX_TMA_VARIANTS entries: the configuration
  * index per variant, -1 where the batch has none.  Synchronises stream. */
 #define CGX_TMA_VARIANTS 40
-#define CGX_TMA_CONFIGS 3
+#define CGX_TMA_CONFIGS 5
 int cgx_batch_autotune(cgx_batch *b, int reps, void *stream, int *chosen);
 /* pin the tile configuration (0 .. CGX_TMA_CONFIGS-1) of one prolongation
  * variant, or of all with variant = -1 (e.g. a saved autotune result);

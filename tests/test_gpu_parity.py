@@ -200,7 +200,7 @@ def test_batched_mixed_pairs_match_per_box_and_oracle(cgx, port, fma):
     st = b.stats()
     assert st["pairs"] == 60 and st["tiles"] > 60
     b.upload()
-    modes = ["batch", "per_box", "graph"] + [f"config{c}" for c in range(3)] + ["autotuned"]
+    modes = ["batch", "per_box", "graph"] + [f"config{c}" for c in range(5)] + ["autotuned"]
     for mode in modes:
         for dst, _, _, init in items:
             dst.tensor.copy_(torch.from_numpy(init))
@@ -211,7 +211,7 @@ def test_batched_mixed_pairs_match_per_box_and_oracle(cgx, port, fma):
             b.launch()
         elif mode == "autotuned":
             chosen = b.autotune(reps=2)
-            assert chosen and all(0 <= c < 3 for c in chosen.values())
+            assert chosen and all(0 <= c < 5 for c in chosen.values())
             for dst, _, _, init in items:  # autotuning ran the batch: start over
                 dst.tensor.copy_(torch.from_numpy(init))
             b.launch()
