@@ -19,6 +19,11 @@ class cgx_array(C.Structure):
     _fields_ = [("data", C.c_void_p), ("padext", C.c_int * 3), ("bbox", C.c_int * 9)]
 
 
+class cgx_pair_box(C.Structure):
+    _fields_ = [("dst_comp", C.c_int), ("src_comp", C.c_int), ("dstbox", C.c_int * 9),
+                ("srcbox", C.c_int * 9)]
+
+
 class CgxError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"cgx error {code}: {msg}")
@@ -53,6 +58,18 @@ lib.cgx_batch_stats.argtypes = [C.c_void_p] + [_P(C.c_int64)] * 4
 lib.cgx_batch_kernels.argtypes = [C.c_void_p, _P(C.c_int)]
 lib.cgx_batch_autotune.argtypes = [C.c_void_p, C.c_int, C.c_void_p, _P(C.c_int)]
 lib.cgx_batch_set_config.argtypes = [C.c_void_p, C.c_int, C.c_int]
+lib.cgx_batch_add_many.argtypes = [C.c_void_p, C.c_int, C.c_int, _P(cgx_array), C.c_int, C.c_void_p,
+                                   C.c_void_p, C.c_int, _P(C.c_double), C.c_void_p, C.c_void_p,
+                                   C.c_double, C.c_int, C.c_int]
+_pb = _P(cgx_pair_box)
+lib.cgx_sched_sync.argtypes = [C.c_int, C.c_void_p, C.c_void_p, _pb, C.c_int, _P(C.c_int)]
+lib.cgx_sched_prolong.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                  C.c_void_p, C.c_int, C.c_int, C.c_int, _pb, C.c_int, _P(C.c_int)]
+lib.cgx_sched_restrict.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                   C.c_int, C.c_int, _pb, C.c_int, _P(C.c_int)]
+lib.cgx_sched_old2new.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                  C.c_void_p, C.c_int, _pb, C.c_int, _P(C.c_int), _pb, C.c_int,
+                                  _P(C.c_int)]
 lib.cgx_graph_begin.argtypes = [C.c_void_p]
 lib.cgx_graph_end.argtypes = [C.c_void_p, _P(C.c_void_p)]
 lib.cgx_graph_launch.argtypes = [C.c_void_p, C.c_void_p]

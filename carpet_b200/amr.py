@@ -150,10 +150,9 @@ class BergerOliger:
         if kind == "sync":
             r, = rots
             arrs = self._tl(l, r, 0)
-            for g in range(st.ngf):
-                for p in h.sync[l]:
-                    b.add(arrs[g][p.dst_comp], [arrs[g][p.src_comp]], [0.0], p.dstbox, p.srcbox,
-                          0.0, 1, 0, op=self.op, cent=self.cent)
+            b.add_many([(arrs[g][p.dst_comp], [arrs[g][p.src_comp]], p.dstbox, p.srcbox)
+                        for g in range(st.ngf) for p in h.sync[l]],
+                       [0.0], 0.0, 1, 0, op=self.op, cent=self.cent)
         elif kind == "prolong":
             rf, rc = rots
             dst = self._tl(l, rf, 0)
@@ -163,19 +162,16 @@ class BergerOliger:
             dtc = 1.0 / 64
             times = [0.0, -dtc, -2 * dtc]
             time = -dtc / 2 if ntl > 1 else 0.0
-            for g in range(st.ngf):
-                for p in h.prolong[l]:
-                    b.add(dst[g][p.dst_comp], [s[g][p.src_comp] for s in srcs], times,
-                          p.dstbox, p.srcbox, time, self.order_space, self.order_time,
-                          op=self.op, cent=self.cent)
+            b.add_many([(dst[g][p.dst_comp], [s[g][p.src_comp] for s in srcs], p.dstbox, p.srcbox)
+                        for g in range(st.ngf) for p in h.prolong[l]],
+                       times, time, self.order_space, self.order_time, op=self.op, cent=self.cent)
         elif kind == "restrict":
             rc, rf = rots
             dst = self._tl(l, rc, 0)
             src = self._tl(l + 1, rf, 0)
-            for g in range(st.ngf):
-                for p in h.restrict[l + 1]:
-                    b.add(dst[g][p.dst_comp], [src[g][p.src_comp]], [0.0], p.dstbox, p.srcbox,
-                          0.0, self.order_space, 0, op=self.op, cent=self.cent)
+            b.add_many([(dst[g][p.dst_comp], [src[g][p.src_comp]], p.dstbox, p.srcbox)
+                        for g in range(st.ngf) for p in h.restrict[l + 1]],
+                       [0.0], 0.0, self.order_space, 0, op=self.op, cent=self.cent)
         b.upload()
         return b
 

@@ -675,6 +675,30 @@ int cgx_batch_add(cgx_batch *b, int op, int cent, const cgx_array *dst, const cg
   return CGX_OK;
 }
 
+int cgx_batch_add_many(cgx_batch *b, int op, int cent, const cgx_array *arrays, int npairs,
+                       const int *dst_idx, const int *src_idx, int nsrc, const double *times,
+                       const int *dstboxes, const int *srcboxes, double time, int order_space,
+                       int order_time) {
+  if (!b || npairs < 0 || nsrc < 1 || nsrc > 3 ||
+      (npairs > 0 && (!arrays || !dst_idx || !src_idx || !dstboxes || !srcboxes)))
+    return fail(CGX_EINVAL, "add_many: bad arguments");
+  b->descs.reserve(b->descs.size() + npairs);
+  cgx_array srcs[3];
+  for (int i = 0; i < npairs; ++i) {
+    for (int t = 0; t < nsrc; ++t) srcs[t] = arrays[src_idx[nsrc * i + t]];
+    Built x;
+    int rc = build(op, cent, &arrays[dst_idx[i]], srcs, times, nsrc, dstboxes + 9 * (size_t)i,
+                   srcboxes + 9 * (size_t)i, nullptr, time, order_space, order_time, &x);
+    if (rc) return rc;
+    b->descs.push_back(x.d);
+    b->bytes.push_back(x.bytes);
+    b->points.push_back(x.points);
+    b->ntiles.push_back(x.ntiles);
+    b->high.push_back(x.d.kind == K_PROLONG_VC && x.d.order >= 7);
+  }
+  return CGX_OK;
+}
+
 int cgx_batch_stats(const cgx_batch *b, int64_t *npairs, int64_t *ntiles, int64_t *dst_points,
                     int64_t *bytes) {
   if (!b) return fail(CGX_EINVAL, "null batch");

@@ -151,7 +151,7 @@ def build_level(box: Box, parts, ghost: int) -> Level:
 
 
 def nested(nlevels: int, npoints, parts=(2, 2, 2), ghost=3, buffer=9, order=5,
-           origin=(0, 0, 0)) -> Hierarchy:
+           origin=(0, 0, 0), native: bool = True) -> Hierarchy:
     """``nlevels`` vertex-centred levels of ``npoints`` points per axis each
     (an int or one per axis, each 1 mod 4), each level covering the central
     half of the next coarser one; ``parts`` splits every level into
@@ -169,7 +169,7 @@ def nested(nlevels: int, npoints, parts=(2, 2, 2), ghost=3, buffer=9, order=5,
         # next level: the central half, (n-1)/4 coarse points in
         lo = [lo[d] + ((n[d] - 1) // 4) * st for d in range(3)]
     h = Hierarchy(levels, ghost, buffer, order)
-    schedule(h)
+    schedule(h, native)
     return h
 
 
@@ -233,12 +233,21 @@ def _restrict_pairs(coarse: Level, fine: Level, ghost: int, buffer: int) -> List
     return pairs
 
 
-def schedule(h: Hierarchy):
+def schedule(h: Hierarchy, native: bool = True):
+    """the sync / boundary-prolongation / restriction lists of every level,
+    built by the library's C++ schedules (``native``) or by the Python
+    restatement in this module (``_sync_pairs`` ...), which the tests compare"""
+    from . import sched
     for l, lev in enumerate(h.levels):
-        h.sync[l] = _sync_pairs(lev)
+        h.sync[l] = sched.sync(lev.comps) if native else _sync_pairs(lev)
         if l > 0:
-            h.prolong[l] = _prolong_pairs(lev, h.levels[l - 1], h.ghost, h.buffer, h.order)
-            h.restrict[l] = _restrict_pairs(h.levels[l - 1], lev, h.ghost, h.buffer)
+            c = h.levels[l - 1]
+            if native:
+                h.prolong[l] = sched.prolong([lev.box], lev.comps, c.comps, h.ghost, h.buffer, h.order)
+                h.restrict[l] = sched.restrict([lev.box], lev.comps, c.comps, h.ghost, h.buffer)
+            else:
+                h.prolong[l] = _prolong_pairs(lev, c, h.ghost, h.buffer, h.order)
+                h.restrict[l] = _restrict_pairs(c, lev, h.ghost, h.buffer)
     check_coverage(h)
 
 

@@ -62,7 +62,9 @@ def _sub_level(lev: Level, box: Box, comps) -> Level:
     return Level(lev.stride, box, comps)
 
 
-def build(spec: MovingSpec, step: int) -> Hierarchy:
+def build(spec: MovingSpec, step: int, native: bool = True) -> Hierarchy:
+    """the hierarchy at a coarse step; schedules from the library's C++
+    (``native``) or from the Python restatement (the tests compare both)"""
     s0 = 2 ** (spec.nlevels - 1)
     box0 = mkbox((0, 0, 0), ((spec.n0 - 1) * s0,) * 3, (s0,) * 3)
     levels = [H.build_level(box0, spec.parts0, spec.ghost)]
@@ -87,6 +89,16 @@ def build(spec: MovingSpec, step: int) -> Hierarchy:
         owners.append(rng)
     h = Hierarchy(levels, spec.ghost, spec.buffer, spec.order)
     h.boxes, h.owners = boxes, owners
+    if native:
+        from . import sched
+        for l, lev in enumerate(levels):
+            h.sync[l] = sched.sync(lev.comps)
+            if l > 0:
+                c = levels[l - 1].comps
+                h.prolong[l] = sched.prolong(boxes[l], lev.comps, c, spec.ghost, spec.buffer, spec.order)
+                h.restrict[l] = sched.restrict(boxes[l], lev.comps, c, spec.ghost, spec.buffer)
+        check(h)
+        return h
     for l, lev in enumerate(levels):
         h.sync[l] = H._sync_pairs(lev)
         if l == 0:
@@ -131,12 +143,19 @@ def _minus_all(a: Box, cut: List[Box]) -> List[Box]:
     return parts
 
 
-def old2new(old: Hierarchy, new: Hierarchy, l: int):
+def old2new(old: Hierarchy, new: Hierarchy, l: int, native: bool = True):
     """the fill of refined level l of ``new``: copy pairs (dst: new component,
     src: old component of level l) over the old interiors, and prolongation
     pairs (src: component of level l-1 of ``new``) for the rest of every new
-    component's exterior."""
+    component's exterior; C++ (``native``) or the Python restatement"""
     assert l > 0
+    if native:
+        from . import sched
+        copies, prols = sched.old2new(new.levels[l].comps, old.levels[l].comps, new.levels[l - 1].comps,
+                                      new.order)
+        want = sum(npoints(cm.exterior) for cm in new.levels[l].comps)
+        assert sum(npoints(p.dstbox) for p in copies + prols) == want, ("old2new coverage", l)
+        return copies, prols
     lnew, lold, coarse = new.levels[l], old.levels[l], new.levels[l - 1]
     cs = coarse.stride
     copies, prols = [], []
@@ -178,13 +197,10 @@ class Regrid:
                 b = Batch()
                 dst, src_old = new_tl(l, tl), old_tl(l, tl)
                 src_coarse = new_tl(l - 1, tl)
-                for g in range(ngf):
-                    for p in copies:
-                        b.add(dst[g][p.dst_comp], [src_old[g][p.src_comp]], [0.0], p.dstbox, p.srcbox,
-                              0.0, 1, 0)
-                    for p in prols:
-                        b.add(dst[g][p.dst_comp], [src_coarse[g][p.src_comp]], [0.0], p.dstbox,
-                              p.srcbox, 0.0, new.order, 0)
+                b.add_many([(dst[g][p.dst_comp], [src_old[g][p.src_comp]], p.dstbox, p.srcbox)
+                            for g in range(ngf) for p in copies], [0.0], 0.0, 1, 0)
+                b.add_many([(dst[g][p.dst_comp], [src_coarse[g][p.src_comp]], p.dstbox, p.srcbox)
+                            for g in range(ngf) for p in prols], [0.0], 0.0, new.order, 0)
                 self.pairs += ngf * (len(copies) + len(prols))
                 self.batches.append(b)
 

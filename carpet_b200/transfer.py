@@ -16,6 +16,7 @@ from __future__ import annotations
 import ctypes as C
 from typing import Optional, Sequence
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -136,6 +137,30 @@ class Batch:
         check(lib.cgx_batch_add(self.h, op, cent, C.byref(d), arr, ts, len(srcs), box9(dstbox),
                                 box9(srcbox), ints3(slab_offset), float(time), int(order_space),
                                 int(order_time)))
+
+    def add_many(self, pairs, times, time, order_space, order_time, op=OP_LAGRANGE, cent=VERTEX):
+        """add a list of (dst Data, [src Data per timelevel], dstbox, srcbox)
+        in one library call (cgx_batch_add_many)"""
+        if not pairs:
+            return
+        index, arrays = {}, []
+
+        def idx(d: Data):
+            k = id(d)
+            if k not in index:
+                index[k] = len(arrays)
+                arrays.append(d)
+            return index[k]
+        nsrc = len(pairs[0][1])
+        di = np.array([idx(p[0]) for p in pairs], dtype=np.int32)
+        si = np.array([[idx(s) for s in p[1]] for p in pairs], dtype=np.int32).reshape(-1)
+        db = np.array([p[2] for p in pairs], dtype=np.int32).reshape(-1)
+        sb = np.array([p[3] for p in pairs], dtype=np.int32).reshape(-1)
+        arr = (cgx_array * len(arrays))(*[a.cgx() for a in arrays])
+        ts = (C.c_double * len(times))(*times)
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        check(lib.cgx_batch_add_many(self.h, op, cent, arr, len(pairs), vp(di), vp(si), nsrc, ts, vp(db),
+                                     vp(sb), float(time), int(order_space), int(order_time)))
 
     def add_raw(self, op, cent, dst: cgx_array, srcs_arr, ts, nsrc, dstbox, srcbox, time,
                 order_space, order_time):

@@ -122,6 +122,16 @@ int cgx_batch_add(cgx_batch *b, int op, int cent, const cgx_array *dst,
                   const int dstbox[9], const int srcbox[9],
                   const int *slab_offset, double time, int order_space,
                   int order_time);
+/* many box-pairs at once (no counterpart in the reference: the loop of
+ * ggf::transfer_from_all, CarpetLib/src/ggf.cc:500-591, over a pair list,
+ * in one call): pair i writes arrays[dst_idx[i]] in dstboxes[9i..] from the
+ * nsrc arrays arrays[src_idx[nsrc*i + t]] in srcboxes[9i..]; every pair
+ * shares op, cent, times, time and the orders.  Stops at the first invalid
+ * pair (the ones before it stay added). */
+int cgx_batch_add_many(cgx_batch *b, int op, int cent, const cgx_array *arrays, int npairs,
+                       const int *dst_idx, const int *src_idx, int nsrc, const double *times,
+                       const int *dstboxes, const int *srcboxes, double time, int order_space,
+                       int order_time);
 /* number of box-pairs, tiles and algorithmic bytes (reads + writes) */
 int cgx_batch_stats(const cgx_batch *b, int64_t *npairs, int64_t *ntiles,
                     int64_t *dst_points, int64_t *bytes);
@@ -149,6 +159,36 @@ int cgx_batch_autotune(cgx_batch *b, int reps, void *stream, int *chosen);
 int cgx_batch_set_config(cgx_batch *b, int variant, int config);
 /* plain per-box launches of the same descriptors (one kernel per pair) */
 int cgx_batch_launch_per_box(cgx_batch *b, void *stream);
+/* ---- host schedules: the send/recv region lists of dh (CarpetLib/src/
+ * dh.cc) for box hierarchies.  Components are given by their interior (the
+ * component's share of its level) and exterior (grown by the ghost zones)
+ * boxes, int[9] each; refined levels by their boxes.  Each call writes up to
+ * max pairs and sets *npairs to the number the schedule has (CGX_ENOMEM when
+ * that is more than max: call again with room for *npairs). */
+typedef struct cgx_pair_box {
+  int dst_comp, src_comp;
+  int dstbox[9], srcbox[9];
+} cgx_pair_box;
+/* ghost sync within a level, dh.cc:837-894 */
+int cgx_sched_sync(int ncomp, const int *interior, const int *exterior, cgx_pair_box *out, int max,
+                   int *npairs);
+/* boundary prolongation of the fine boxes' outer ghost+buffer layers from
+ * the coarse components, send boxes grown by order/2, dh.cc:896-977 */
+int cgx_sched_prolong(int nbox, const int *fboxes, int nfcomp, const int *finterior, int nccomp,
+                      const int *cinterior, const int *cexterior, int ghost, int buffer, int order,
+                      cgx_pair_box *out, int max, int *npairs);
+/* restriction of the coarse points under the fine boxes' active regions,
+ * dh.cc:981-1088 (dst: coarse component, src: fine component) */
+int cgx_sched_restrict(int nbox, const int *fboxes, int nfcomp, const int *finterior, int nccomp,
+                       const int *cinterior, int ghost, int buffer, cgx_pair_box *out, int max,
+                       int *npairs);
+/* regrid fill of one refined level, dh.cc:1717-1830: copies from the old
+ * components' interiors, prolongation from the coarse components for the
+ * rest of every new component's exterior */
+int cgx_sched_old2new(int nnew, const int *new_exterior, int nold, const int *old_interior, int nccomp,
+                      const int *cinterior, const int *cexterior, int order, cgx_pair_box *copies,
+                      int max_copies, int *ncopies, cgx_pair_box *prols, int max_prols, int *nprols);
+
 /* device status word of the last launches: 0 or a CGX_E* code */
 int cgx_batch_check(cgx_batch *b, void *stream);
 
