@@ -509,11 +509,10 @@ def main():
         return
 
     import torch
+    from carpet_b200 import replicas
     if world > 1:
-        import datetime
-        import torch.distributed as dist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        replicas.init("nccl", timeout_s=120)
     import carpet_b200 as cb
     from carpet_b200.amr import BergerOliger, Storage
     from carpet_b200.hierarchy import nested
@@ -549,8 +548,7 @@ def main():
         graphs.append(g)
 
     def barrier():
-        if world > 1:
-            torch.distributed.barrier()
+        replicas.barrier()
         torch.cuda.synchronize()
 
     # warm-up, then K timed steps
@@ -565,15 +563,11 @@ def main():
         e1.record(stream)
         stream.synchronize()
     barrier()
-    ms = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.max_over_ranks(e0.elapsed_time(e1) / args.steps)
     for b in bo.batches.values():
         b.check(stream)
-    value = bytes_step * world / (ms * 1e-3) / 1e9
-    fine_pts = points_step * world / (ms * 1e-3)
+    value = replicas.job_throughput(bytes_step, world, ms) / 1e9
+    fine_pts = replicas.job_throughput(points_step, world, ms)
 
     # per-launch timing of every phase (same stream, no graph): each phase
     # is a homogeneous batch, i.e. one kernel; the dominant kernel is the
@@ -655,12 +649,8 @@ def main():
             e2e_step(s + 1)
         b_.record(stream)
         stream.synchronize()
-        ems = a.elapsed_time(b_) / n_e2e
-        if world > 1:
-            t = torch.tensor([ems], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ems = float(t.item())
-        e2e = {"value": round(bytes_step * world / (ems * 1e-3) / 1e9, 3), "unit": "GB/s",
+        ems = replicas.max_over_ranks(a.elapsed_time(b_) / n_e2e)
+        e2e = {"value": round(replicas.job_throughput(bytes_step, world, ems) / 1e9, 3), "unit": "GB/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "ms_per_step": round(ems, 3)}
 
@@ -721,10 +711,8 @@ def main():
             "batched_uneven": batched_uneven, "moving_boxes": moving_boxes,
         }
         print(json.dumps(out))
-    for g in graphs:
-        del g
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    del graphs
+    replicas.finish()
 
 
 if __name__ == "__main__":
