@@ -367,7 +367,7 @@ def uneven(steps: int, warmup: int, fp: str):
     pairs = uneven_pairs(uneven_specs(seed=3, npairs=256, ext=(16, 96)), seed=4)
     b = uneven_batch(pairs)
     st = b.stats()
-    tuned = b.autotune(reps=3)
+    tuned = b.autotune(reps=5)
     s = torch.cuda.Stream()
     g = cb.Graph()
     with g.capture(s):
@@ -426,7 +426,7 @@ def moving(ngf: int, fp: str, steps: int):
     # one coarse step
     bo = BergerOliger(h0, st, order_space=5, order_time=2)
     keys = bo.step_phases()
-    tuned = bo.autotune(keys, reps=1)
+    tuned = bo.autotune(keys, reps=3)
     g = cb.Graph()
     with g.capture(s):
         bo.run(keys, s)
@@ -529,7 +529,7 @@ def main():
     tuned = {}
     if not args.no_tune:
         for keys in steps3:
-            for k, v in bo.autotune(keys, reps=2).items():
+            for k, v in bo.autotune(keys, reps=5).items():
                 if v:
                     tuned[f"{k[0]}-ntl{k[3]}"] = v
     stats = [bo.stats(k) for k in steps3]

@@ -826,8 +826,8 @@ int cgx_batch_launch(cgx_batch *b, void *stream) {
 
 // The autotuner: for every TMA prolongation variant present, run its
 // segment of the batch in each tile configuration (one untimed launch, then
-// `reps` timed with events on the stream) and keep the fastest; then upload
-// with the choices.  Repeated launches of a batch write the same values
+// `reps` launches timed one by one with events; the median scores) and keep
+// the fastest; then upload with the choices.  Repeated launches of a batch write the same values
 // (pairs write disjoint points and read none of them), so tuning on the
 // caller's own data is safe.
 static_assert(CGX_TMA_VARIANTS == TV_COUNT && CGX_TMA_CONFIGS == TMA_NCFG, "tuning constants of the C-ABI");
@@ -838,10 +838,16 @@ int cgx_batch_autotune(cgx_batch *b, int reps, void *stream, int *chosen) {
   if (rc) return rc;
   bool present[TV_COUNT];
   for (int v = 0; v < TV_COUNT; ++v) present[v] = b->seg[v + 1] > b->seg[v];
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  cudaError_t e = cudaEventCreate(&e0);
-  if (e == cudaSuccess) e = cudaEventCreate(&e1);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
+  // each launch timed on its own; a configuration scores the median
+  std::vector<cudaEvent_t> ev(2 * (size_t)reps, nullptr);
+  cudaError_t e = cudaSuccess;
+  for (auto &x : ev)
+    if (e == cudaSuccess) e = cudaEventCreate(&x);
+  if (e != cudaSuccess) {
+    for (auto x : ev)
+      if (x) cudaEventDestroy(x);
+    return cuda_fail(e, "cudaEventCreate");
+  }
   auto run_segment = [&](int v) {
     long long sg[NSEG + 1];
     for (int i = 0; i <= NSEG; ++i) sg[i] = i <= v ? b->seg[v] : b->seg[v + 1];
@@ -858,22 +864,26 @@ int cgx_batch_autotune(cgx_batch *b, int reps, void *stream, int *chosen) {
       b->tma_cfg[v] = c;
       if ((rc = cgx_batch_upload(b, stream))) break;
       if ((rc = run_segment(v))) break;
-      e = cudaEventRecord(e0, s);
-      for (int r = 0; r < reps && rc == CGX_OK && e == cudaSuccess; ++r) rc = run_segment(v);
-      if (e == cudaSuccess) e = cudaEventRecord(e1, s);
-      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-      float ms = 0.f;
-      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      for (int r = 0; r < reps && rc == CGX_OK && e == cudaSuccess; ++r) {
+        e = cudaEventRecord(ev[2 * r], s);
+        if (e == cudaSuccess) rc = run_segment(v);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[2 * r + 1], s);
+      }
+      if (e == cudaSuccess) e = cudaEventSynchronize(ev[2 * reps - 1]);
+      std::vector<float> t((size_t)reps, 0.f);
+      for (int r = 0; r < reps && e == cudaSuccess; ++r) e = cudaEventElapsedTime(&t[r], ev[2 * r], ev[2 * r + 1]);
       if (e != cudaSuccess) rc = cuda_fail(e, "autotune timing");
-      if (rc == CGX_OK && (c == 0 || ms < best_ms)) {
+      if (rc) break;
+      std::sort(t.begin(), t.end());
+      const float ms = t[(size_t)reps / 2];
+      if (c == 0 || ms < best_ms) {
         best = c;
         best_ms = ms;
       }
     }
     b->tma_cfg[v] = best;
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  for (auto x : ev) cudaEventDestroy(x);
   if (rc) return rc;
   if (chosen)
     for (int v = 0; v < TV_COUNT; ++v) chosen[v] = present[v] ? b->tma_cfg[v] : -1;

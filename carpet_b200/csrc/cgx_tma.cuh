@@ -135,6 +135,7 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
   using G = TGeom<F, PYC>;
   using S = TSmem<F, NTL, PYC, NB>;
   constexpr int LO = F::LO, HI = F::HI, Q = G::Q;
+  constexpr bool SPLIT = NTL == 1;
   const int tid = threadIdx.x;
   const int ptx = d.ptx, ptyc = d.ptyc, pty = 2 * ptyc - 1;
   const int BX = d.bx, BY = d.by;
@@ -189,9 +190,11 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
   }
   auto xpass = [&](int slot, double *__restrict__ xr) {
     const double *__restrict__ cs = coarse + slot * NTL * G::TLS - LO;
+    // with SPLIT every thread runs all IT items (the ones past the plane's
+    // count read the slot's first points and write the spare row)
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
-      if (k * NT < count) { // uniform
+      if (SPLIT || k * NT < count) { // uniform
         const double *row = cs + xsrc[k];
         auto get = [&](int m) { return row[m]; };
         const double xe = F::template first<FMA>(0, get);
@@ -263,26 +266,43 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
     for (int p = 0; p < PD; ++p)
       if (p < nplanes) issue(p);
   }
+  // Iteration i: stage plane i + PD; wait for plane i and run its x pass
+  // (DX: i < nplanes); run the y/z pass of plane i - 1 (DY: i >= 1).  The
+  // barrier also reduces the waits' failures (__syncthreads_or).  With
+  // SPLIT (one timelevel: a short loop body) the whole groups of Q
+  // iterations run without per-iteration checks and a second unrolled copy
+  // handles the last ones; the longer multi-timelevel bodies keep one
+  // unrolled copy with the checks (two copies cost more in instruction
+  // fetch than the checks).
   bool ok = true;
-  auto iteration = [&](auto Ut, int i) {
+  auto iteration = [&](auto Ut, int i, auto DX, auto DY) {
+    constexpr bool X = decltype(DX)::value, Y = decltype(DY)::value;
+    if (!ok) return; // uniform: a wait gave up
     if (tid == 0 && i + PD < nplanes) issue(i + PD);
-    if (i < nplanes) {
-      const unsigned g = g0 + (unsigned)i;
-      if (!mbar_wait_bounded(&ring.bars[g % NB], (g / NB) & 1)) *ring.abort = 1;
+    const unsigned g = g0 + (unsigned)i;
+    const int fail = X ? !mbar_wait_bounded(&ring.bars[g % NB], (g / NB) & 1) : 0;
+    if (__syncthreads_or(fail)) {
+      if (tid == 0) *ring.abort = 1;
+      ok = false;
+      return;
     }
-    __syncthreads();
-    if (*ring.abort) { ok = false; return; }
-    if (i < nplanes) xpass((int)((g0 + (unsigned)i) % NB), xrows + (i & 1) * S::xbuf);
-    if (i >= 1) yzpass(Ut, i - 1, xrows + ((i - 1) & 1) * S::xbuf);
+    if (X) xpass((int)(g % NB), xrows + (i & 1) * S::xbuf);
+    if (Y) yzpass(Ut, i - 1, xrows + ((i - 1) & 1) * S::xbuf);
   };
-  iteration(std::integral_constant<int, Q - 1>(), 0);
-  for (int i0 = 1; ok && i0 <= nplanes; i0 += Q) {
+  using T_ = std::true_type;
+  using F_ = std::false_type;
+  iteration(std::integral_constant<int, Q - 1>(), 0, T_(), F_());
+  // whole groups of Q iterations with both passes, then the last ones
+  int i0 = 1;
+  if (SPLIT)
+    for (; ok && i0 + Q <= nplanes; i0 += Q)
+      static_for<Q>([&](auto Ut) { iteration(Ut, i0 + decltype(Ut)::value, T_(), T_()); });
+  for (; ok && i0 <= nplanes; i0 += Q)
     static_for<Q>([&](auto Ut) {
-      constexpr int u = decltype(Ut)::value;
-      const int i = i0 + u;
-      if (ok && i <= nplanes) iteration(std::integral_constant<int, u>(), i);
+      const int i = i0 + decltype(Ut)::value;
+      if (ok && i < nplanes) iteration(Ut, i, T_(), T_());
+      else if (ok && i == nplanes) iteration(Ut, i, F_(), T_());
     });
-  }
   if (!ok) {
     // a wait gave up: wait (bounded) for every plane staged, so that no
     // copy lands after the CTA has left
