@@ -271,9 +271,7 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
   // barrier also reduces the waits' failures (__syncthreads_or).  With
   // SPLIT (one timelevel: a short loop body) the whole groups of Q
   // iterations run without per-iteration checks and a second unrolled copy
-  // handles the last ones; the longer multi-timelevel bodies keep one
-  // unrolled copy with the checks (two copies cost more in instruction
-  // fetch than the checks).
+  // handles the last ones.
   bool ok = true;
   auto iteration = [&](auto Ut, int i, auto DX, auto DY) {
     constexpr bool X = decltype(DX)::value, Y = decltype(DY)::value;
@@ -289,20 +287,42 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
     if (X) xpass((int)(g % NB), xrows + (i & 1) * S::xbuf);
     if (Y) yzpass(Ut, i - 1, xrows + ((i - 1) & 1) * S::xbuf);
   };
+  // the same iteration with run-time checks, one unrolled copy: the loop of
+  // the multi-timelevel variants, whose long bodies make a second unrolled
+  // copy (and its register allocation) cost more than the checks
+  auto iteration_rt = [&](auto Ut, int i) {
+    if (tid == 0 && i + PD < nplanes) issue(i + PD);
+    const unsigned g = g0 + (unsigned)i;
+    if (i < nplanes && !mbar_wait_bounded(&ring.bars[g % NB], (g / NB) & 1)) *ring.abort = 1;
+    __syncthreads();
+    if (*ring.abort) {
+      ok = false;
+      return;
+    }
+    if (i < nplanes) xpass((int)(g % NB), xrows + (i & 1) * S::xbuf);
+    if (i >= 1) yzpass(Ut, i - 1, xrows + ((i - 1) & 1) * S::xbuf);
+  };
   using T_ = std::true_type;
   using F_ = std::false_type;
-  iteration(std::integral_constant<int, Q - 1>(), 0, T_(), F_());
-  // whole groups of Q iterations with both passes, then the last ones
   int i0 = 1;
-  if (SPLIT)
+  if (SPLIT) {
+    iteration(std::integral_constant<int, Q - 1>(), 0, T_(), F_());
+    // whole groups of Q iterations with both passes, then the last ones
     for (; ok && i0 + Q <= nplanes; i0 += Q)
       static_for<Q>([&](auto Ut) { iteration(Ut, i0 + decltype(Ut)::value, T_(), T_()); });
-  for (; ok && i0 <= nplanes; i0 += Q)
     static_for<Q>([&](auto Ut) {
       const int i = i0 + decltype(Ut)::value;
       if (ok && i < nplanes) iteration(Ut, i, T_(), T_());
       else if (ok && i == nplanes) iteration(Ut, i, F_(), T_());
     });
+  } else {
+    iteration_rt(std::integral_constant<int, Q - 1>(), 0);
+    for (; ok && i0 <= nplanes; i0 += Q)
+      static_for<Q>([&](auto Ut) {
+        const int i = i0 + decltype(Ut)::value;
+        if (ok && i <= nplanes) iteration_rt(Ut, i);
+      });
+  }
   if (!ok) {
     // a wait gave up: wait (bounded) for every plane staged, so that no
     // copy lands after the CTA has left
