@@ -14,7 +14,8 @@ value        algorithmic GB/s of the batched form (one persistent kernel per
              phase, the step replayed as CUDA graphs), inputs resident in HBM
 e2e          the same step through the public API with the grid data in
              pinned host memory: H2D of every array the step reads and D2H of
-             every array it writes, inside the timed region
+             every array it writes, inside the timed region (two device
+             copies alternate so copy-in, kernels and copy-out overlap)
 plain        the plain per-box form (one launch per box-pair), same step
 roofline     the dominant kernel (the phase kind with the largest share of
              the step): its algorithmic bytes per launch / its CUDA-event time
@@ -526,10 +527,11 @@ def main():
     for keys in steps3:
         for k in keys:
             bo.batch(k)
-    tuned = {}
+    tuned, tuned_by_key = {}, {}
     if not args.no_tune:
         for keys in steps3:
             for k, v in bo.autotune(keys, reps=5).items():
+                tuned_by_key[k] = v
                 if v:
                     tuned[f"{k[0]}-ntl{k[3]}"] = v
     stats = [bo.stats(k) for k in steps3]
@@ -618,41 +620,82 @@ def main():
                  "ms_per_step": round(pms, 3), "launches_per_step": stats[0]["pairs"]}
 
     # end to end: grid data in pinned host memory; every step copies in all
-    # it reads and copies out all it writes (whole levels per timelevel)
+    # it reads and copies out all it writes (whole levels per timelevel).
+    # Two device copies of the hierarchy alternate, so that a step's copy-in
+    # overlaps the previous step's transfers and copy-out (the two copy
+    # directions and the kernels run on three streams).
     e2e = None
     if not args.no_e2e:
         host = [[torch.empty_like(p, device="cpu").pin_memory() for p in lp] for lp in st.pools]
         for lp, hp in zip(st.pools, host):
             for p, q in zip(lp, hp):
                 q.copy_(p)
+        hout = [[torch.empty_like(lp[0], device="cpu").pin_memory() for lp in st.pools] for _ in range(2)]
         h2d = sum(p.numel() * 8 for lp in st.pools for p in lp)
         d2h = sum(lp[0].numel() * 8 for lp in st.pools)
-        n_e2e = max(2, min(args.steps, 4))
+        stB = Storage(h, args.ngf, 3)
+        for la, lb in zip(st.pools, stB.pools):
+            for p, q in zip(la, lb):
+                q.copy_(p)
+        boB = BergerOliger(h, stB, order_space=5, order_time=2)
+        stepsB = [boB.step_phases() for _ in range(3)]
+        for keys in stepsB:
+            for k in keys:
+                for v, c in tuned_by_key.get(k, {}).items():
+                    boB.batch(k).set_config(c, v)
+                boB.batch(k).upload()
+        graphsB = []
+        for keys in stepsB:
+            g = cb.Graph()
+            with g.capture(stream):
+                boB.run(keys, stream)
+            graphsB.append(g)
+        torch.cuda.synchronize()
+        bufs = [(st, bo, graphs), (stB, boB, graphsB)]
+        s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+        in_done = [torch.cuda.Event() for _ in range(2)]
+        comp_done = [torch.cuda.Event() for _ in range(2)]
+        out_done = [torch.cuda.Event() for _ in range(2)]
+        used = [False, False]
+        n_e2e = max(4, min(2 * args.steps, 8))
 
         def e2e_step(s):
-            keys = steps3[s % 3]
-            with torch.cuda.stream(stream):
-                for lp, hp in zip(st.pools, host):
+            x = s % 2
+            sto, bx, gr = bufs[x]
+            if used[x]:
+                s_in.wait_event(out_done[x])  # the buffer's last step is copied out
+            with torch.cuda.stream(s_in):
+                for lp, hp in zip(sto.pools, host):
                     for p, q in zip(lp, hp):
                         p.copy_(q, non_blocking=True)
-                graphs[s % 3].launch(stream)
-                for l, (lp, hp) in enumerate(zip(st.pools, host)):
-                    i = bo.pool_index(bo.rot[l], 0)
-                    hp[i].copy_(lp[i], non_blocking=True)
-            return keys
+            in_done[x].record(s_in)
+            stream.wait_event(in_done[x])
+            gr[(s // 2) % 3].launch(stream)
+            comp_done[x].record(stream)
+            s_out.wait_event(comp_done[x])
+            with torch.cuda.stream(s_out):
+                for l, lp in enumerate(sto.pools):
+                    hout[x][l].copy_(lp[bx.pool_index(bx.rot[l], 0)], non_blocking=True)
+            out_done[x].record(s_out)
+            used[x] = True
 
-        e2e_step(0)
-        stream.synchronize()
+        for s in range(2):
+            e2e_step(s)
+        torch.cuda.synchronize()
         a, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
+        a.record(s_in)
         for s in range(n_e2e):
-            e2e_step(s + 1)
-        b_.record(stream)
-        stream.synchronize()
+            e2e_step(s + 2)
+        b_.record(s_out)
+        torch.cuda.synchronize()
         ems = replicas.max_over_ranks(a.elapsed_time(b_) / n_e2e)
         e2e = {"value": round(replicas.job_throughput(bytes_step, world, ems) / 1e9, 3), "unit": "GB/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "ms_per_step": round(ems, 3)}
+               "ms_per_step": round(ems, 3), "steps": n_e2e,
+               "pipelining": "two device copies alternate; copy-in, kernels, copy-out on three streams"}
+        for b in boB.batches.values():
+            b.check(stream)
+        del graphsB
 
     cpu = None
     if rank == 0 and not args.no_cpu:
