@@ -73,6 +73,8 @@ def parse():
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--serve-seconds", type=float, default=1.0)
     p.add_argument("--no-tune", action="store_true", help="default tile configurations")
+    p.add_argument("--tile-config", type=int, default=None,
+                   help="pin every prolongation variant to this tile configuration instead of tuning")
     p.add_argument("--no-uneven", action="store_true", help="skip the batched uneven section")
     p.add_argument("--moving", action="store_true",
                    help="add the moving-box section (~80 GB on the device, minutes)")
@@ -528,7 +530,14 @@ def main():
         for k in keys:
             bo.batch(k)
     tuned, tuned_by_key = {}, {}
-    if not args.no_tune:
+    if args.tile_config is not None:
+        for keys in steps3:
+            for k in keys:
+                bo.batch(k).set_config(args.tile_config)
+                bo.batch(k).upload()
+                tuned_by_key[k] = {v: args.tile_config for v in range(40)}
+        tuned = {"all": {0: args.tile_config}}
+    elif not args.no_tune:
         for keys in steps3:
             for k, v in bo.autotune(keys, reps=5).items():
                 tuned_by_key[k] = v
