@@ -106,6 +106,15 @@ class Port:
         self._op(self.lib.cgxo_restrict_3d_cc_rf2, (int(fma),), src, srcbbox, dst,
                  dstbbox, reg, reg)
 
+    def restrict_3d_cc_ho_rf2(self, order, src, srcbbox, dst, dstbbox, reg, fma=False):
+        """restrict_3d_cc_o3_rf2 (order 3) / restrict_3d_cc_o5_rf2 (order 5)"""
+        fn = {3: self.lib.cgxo_restrict_3d_cc_o3_rf2, 5: self.lib.cgxo_restrict_3d_cc_o5_rf2}[order]
+        self._op(fn, (int(fma),), src, srcbbox, dst, dstbbox, reg, reg)
+
+    def set_restriction(self, use_higher_order: bool, order: int = 1):
+        """the use_higher_order_restriction / restriction_order_space parameters"""
+        self.lib.cgxo_set_restriction(int(use_higher_order), int(order))
+
     def _ti(self, fn, srcs, times, srcbbox, dst, dstbbox, reg, t, fma):
         pre = [int(fma)]
         for s, ts in zip(srcs, times):
@@ -203,6 +212,10 @@ class Ref:
     def restrict_3d_cc_rf2(self, src, srcbbox, dst, dstbbox, reg):
         self._op(self.lib.cgxref_restrict_3d_cc_rf2, (), src, srcbbox, dst, dstbbox,
                  reg, reg)
+
+    def restrict_3d_cc_ho_rf2(self, order, src, srcbbox, dst, dstbbox, reg):
+        fn = {3: self.lib.cgxref_restrict_3d_cc_o3_rf2, 5: self.lib.cgxref_restrict_3d_cc_o5_rf2}[order]
+        self._op(fn, (), src, srcbbox, dst, dstbbox, reg, reg)
 
     def _ti(self, fn, srcs, times, srcbbox, dst, dstbbox, reg, t):
         pre = []

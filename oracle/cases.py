@@ -109,9 +109,11 @@ def vc_restrict_case(rng, fine_stride=1, max_ext=9, kind="normal"):
     return dict(src=src, srcbbox=srcbbox, dst=dst, dstbbox=dstbbox, reg=reg)
 
 
-def cc_restrict_case(rng, half=1, max_ext=9, kind="normal"):
+def cc_restrict_case(rng, half=1, max_ext=9, kind="normal", reach=(0, 0)):
     """Cell-centred averaging: coarse cells (stride 4h at 4h*n + 2h) over
-    fine cells (stride 2h at 2h*m + h)."""
+    fine cells (stride 2h at 2h*m + h); ``reach`` = fine cells the stencil
+    needs below / above a coarse cell's two children (the higher-order
+    restrictions: (1, 1) for order 3, (2, 2) for order 5)."""
     h = half
     fs, cs = 2 * h, 4 * h
     ext = rng.integers(1, max_ext + 1, 3)
@@ -120,8 +122,8 @@ def cc_restrict_case(rng, half=1, max_ext=9, kind="normal"):
     up = lo + (ext - 1) * cs
     reg = _box(lo, up, (cs,) * 3)
     # fine children of coarse cell c are c - h and c + h
-    slo = lo - h - rng.integers(0, 3, 3) * fs
-    sup = up + h + rng.integers(0, 3, 3) * fs
+    slo = lo - h - (reach[0] + rng.integers(0, 3, 3)) * fs
+    sup = up + h + (reach[1] + rng.integers(0, 3, 3)) * fs
     srcbbox = _box(slo, sup, (fs,) * 3)
     dlo = lo - rng.integers(0, 3, 3) * cs
     dup = up + rng.integers(0, 3, 3) * cs

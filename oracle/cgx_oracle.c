@@ -600,6 +600,120 @@ int cgxo_restrict_3d_cc_rf2(int fma_, const double *src, const int *srcpadext,
 }
 
 /* ------------------------------------------------------------------ */
+/* Higher-order cell-centred restriction, selected by CarpetLib's      */
+/* use_higher_order_restriction / restriction_order_space parameters   */
+/* (data.cc:1061-1097); cgxo_set_restriction mirrors them.             */
+
+static int g_ho_restrict = 0, g_restrict_order = 1;
+
+int cgxo_set_restriction(int use_higher_order, int order) {
+  g_ho_restrict = use_higher_order != 0;
+  g_restrict_order = order;
+  return CGXO_OK;
+}
+
+/* region set-up shared by the cc restrictions: offsets of the region's
+ * first fine cell (srcoff) and coarse point (dstoff); the source must hold
+ * fine cells lo..hi around every coarse point (taps relative to 2i) */
+static int cc_restrict_region(const char *who, const int *srcbbox_, const int *dstbbox_,
+                              const int *regbbox_, const int *srcext, int lo, int hi,
+                              int *regext, int *srcoff, int *dstoff) {
+  box_t srcbbox = mkbox(srcbbox_), dstbbox = mkbox(dstbbox_), reg = mkbox(regbbox_);
+  for (int d = 0; d < 3; ++d) {
+    if (srcbbox.str[d] >= reg.str[d] || dstbbox.str[d] != reg.str[d])
+      return fail(CGXO_EINVAL, "%s: strides disagree", who);
+    if (2 * srcbbox.str[d] != dstbbox.str[d])
+      return fail(CGXO_EINVAL, "%s: destination strides are not twice the source strides", who);
+  }
+  if (box_empty(&reg)) return fail(CGXO_EINVAL, "%s: region extent is empty", who);
+  if (!box_in(&reg, &dstbbox))
+    return fail(CGXO_EINVAL, "%s: region extent is not contained in array extent", who);
+  for (int d = 0; d < 3; ++d) {
+    regext[d] = box_size(&reg, d);
+    int h = srcbbox.str[d] / 2;
+    if (srcbbox.str[d] % 2 || (reg.lo[d] - srcbbox.lo[d] - h) % srcbbox.str[d] ||
+        (reg.lo[d] - dstbbox.lo[d]) % dstbbox.str[d])
+      return fail(CGXO_EINVAL, "%s: region not aligned", who);
+    srcoff[d] = (reg.lo[d] - srcbbox.lo[d] - h) / srcbbox.str[d];
+    dstoff[d] = (reg.lo[d] - dstbbox.lo[d]) / dstbbox.str[d];
+    /* every tap inside the source (the stencil's own reach, :128-144) */
+    if (srcoff[d] + lo < 0 || srcoff[d] + 2 * (regext[d] - 1) + hi >= srcext[d])
+      return fail(CGXO_EINVAL, "%s: stencil reaches outside the source array", who);
+  }
+  return CGXO_OK;
+}
+
+/* restrict_3d_cc_o3_rf2, CarpetLib/src/restrict_3d_cc_o3_rf2.cc:33-229:
+ * the 4x4x4 fine cells at 2i-1..2i+2 (per axis), weight c_a c_b c_c / 4096
+ * with c = (-1, 9, 9, -1) (f1..f4 = 1, 9, 81, 729 over 4096, :114-119),
+ * summed left to right with x fastest, then y, then z (:147-211) */
+int cgxo_restrict_3d_cc_o3_rf2(int fma_, const double *src, const int *srcpadext,
+                               const int *srcext, double *dst, const int *dstpadext,
+                               const int *dstext, const int *srcbbox, const int *dstbbox,
+                               const int *srcregbbox, const int *regbbox) {
+  (void)srcregbbox; (void)dstext;
+  int regext[3], srcoff[3], dstoff[3], rc;
+  if ((rc = cc_restrict_region("restrict_3d_cc_o3_rf2", srcbbox, dstbbox, regbbox, srcext, -1, 2,
+                               regext, srcoff, dstoff)))
+    return rc;
+  static const double c1[4] = {-1, 9, 9, -1};
+  double w[64];
+  for (int c = 0; c < 4; ++c)
+    for (int b = 0; b < 4; ++b)
+      for (int a = 0; a < 4; ++a) w[(c * 4 + b) * 4 + a] = (c1[a] * c1[b] * c1[c]) / 4096.0;
+  for (int k = 0; k < regext[2]; ++k)
+    for (int j = 0; j < regext[1]; ++j)
+      for (int i = 0; i < regext[0]; ++i) {
+        const int x0 = srcoff[0] + 2 * i - 1, y0 = srcoff[1] + 2 * j - 1, z0 = srcoff[2] + 2 * k - 1;
+        double res = w[0] * src[IDX(x0, y0, z0, srcpadext)];
+        for (int m = 1; m < 64; ++m)
+          res = madd(fma_, w[m], src[IDX(x0 + (m & 3), y0 + ((m >> 2) & 3), z0 + (m >> 4), srcpadext)], res);
+        dst[IDX(dstoff[0] + i, dstoff[1] + j, dstoff[2] + k, dstpadext)] = res;
+      }
+  return CGXO_OK;
+}
+
+/* restrict_3d_cc_o5_rf2, CarpetLib/src/restrict_3d_cc_o5_rf2.cc:36-78,
+ * 159-193: separable, restrict3 over planes 2k-2..2k+3 of restrict2 over
+ * rows of restrict1 over cells 2i-2..2i+3, each a left-to-right sum with
+ * weights (3, -25, 150, 150, -25, 3) / 256 */
+static const double o5w[6] = {3.0 / 256, -25.0 / 256, 150.0 / 256, 150.0 / 256, -25.0 / 256, 3.0 / 256};
+
+static double o5_line(int fma_, const double *p, long long stride) {
+  double r = o5w[0] * p[-2 * stride];
+  for (int m = 1; m < 6; ++m) r = madd(fma_, o5w[m], p[(m - 2) * stride], r);
+  return r;
+}
+
+int cgxo_restrict_3d_cc_o5_rf2(int fma_, const double *src, const int *srcpadext,
+                               const int *srcext, double *dst, const int *dstpadext,
+                               const int *dstext, const int *srcbbox, const int *dstbbox,
+                               const int *srcregbbox, const int *regbbox) {
+  (void)srcregbbox; (void)dstext;
+  int regext[3], srcoff[3], dstoff[3], rc;
+  if ((rc = cc_restrict_region("restrict_3d_cc_o5_rf2", srcbbox, dstbbox, regbbox, srcext, -2, 3,
+                               regext, srcoff, dstoff)))
+    return rc;
+  const long long sy = srcpadext[0], sz = (long long)srcpadext[0] * srcpadext[1];
+  for (int k = 0; k < regext[2]; ++k)
+    for (int j = 0; j < regext[1]; ++j)
+      for (int i = 0; i < regext[0]; ++i) {
+        const double *p = src + IDX(srcoff[0] + 2 * i, srcoff[1] + 2 * j, srcoff[2] + 2 * k, srcpadext);
+        double r3 = 0;
+        for (int c = 0; c < 6; ++c) {
+          double r2 = 0;
+          for (int b = 0; b < 6; ++b) {
+            const double r1 = o5_line(fma_, p + (c - 2) * sz + (b - 2) * sy, 1);
+            r2 = b ? madd(fma_, o5w[b], r1, r2) : o5w[0] * r1;
+          }
+          r3 = c ? madd(fma_, o5w[c], r2, r3) : o5w[0] * r2;
+        }
+        dst[IDX(dstoff[0] + i, dstoff[1] + j, dstoff[2] + k, dstpadext)] = r3;
+      }
+  return CGXO_OK;
+}
+
+/* ------------------------------------------------------------------ */
 /* Time interpolation                                                 */
 
 static int ti_region(const box_t *srcbbox, const box_t *dstbbox, const box_t *reg,
@@ -842,9 +956,23 @@ static int transfer_p_r(int fma_, int op, int cent, double *dst,
         return cgxo_restrict_3d_rf2(src, srcpadext, srcext, dst, dstpadext, dstext,
                                     srcbbox, dstbbox, srcbox, dstbox);
       }
-      if (cent == cell_centered)
+      if (cent == cell_centered) {
+        /* data.cc:1061-1097: the parameters pick the stencil, except for
+         * the ENO and WENO transport operators */
+        if (g_ho_restrict && op != op_ENO && op != op_WENO) {
+          if (g_restrict_order == 3)
+            return cgxo_restrict_3d_cc_o3_rf2(fma_, src, srcpadext, srcext, dst, dstpadext,
+                                              dstext, srcbbox, dstbbox, srcbox, dstbox);
+          if (g_restrict_order == 5)
+            return cgxo_restrict_3d_cc_o5_rf2(fma_, src, srcpadext, srcext, dst, dstpadext,
+                                              dstext, srcbbox, dstbbox, srcbox, dstbox);
+          if (g_restrict_order != 1)
+            return fail(CGXO_EINVAL, "There is no restriction stencil with restriction_order_space==%d",
+                        g_restrict_order);
+        }
         return cgxo_restrict_3d_cc_rf2(fma_, src, srcpadext, srcext, dst, dstpadext,
                                        dstext, srcbbox, dstbbox, srcbox, dstbox);
+      }
       return fail(CGXO_EINVAL, "transfer_restrict: bad centering");
     }
     return fail(CGXO_EUNSUPPORTED, "transfer_restrict: operator outside the restated set");

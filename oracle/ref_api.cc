@@ -157,6 +157,16 @@ int cgxref_restrict_3d_cc_rf2(OPARGS) {
   return guarded([&] { restrict_3d_cc_rf2<double>(OPCALL, nullptr); });
 }
 
+// restrict_3d_cc_o3_rf2 / restrict_3d_cc_o5_rf2
+// (CarpetLib/src/restrict_3d_cc_o3_rf2.cc:33, restrict_3d_cc_o5_rf2.cc:79);
+// CarpetLib calls them without call_operator (data.cc:1065-1085).
+int cgxref_restrict_3d_cc_o3_rf2(OPARGS) {
+  return guarded([&] { restrict_3d_cc_o3_rf2<double>(OPCALL, nullptr); });
+}
+int cgxref_restrict_3d_cc_o5_rf2(OPARGS) {
+  return guarded([&] { restrict_3d_cc_o5_rf2<double>(OPCALL, nullptr); });
+}
+
 #define TIARGS                                                                 \
   const int *srcpadext, const int *srcext, double *dst, double t,              \
       const int *dstpadext, const int *dstext, const int *srcbbox,             \

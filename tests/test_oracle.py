@@ -276,3 +276,59 @@ def test_transfer_composes_space_then_time(port):
     with pytest.raises(OracleError):
         port.transfer(OP_SYNC, VERTEX, d, c["dstbbox"], srcs, c["srcbbox"], times,
                       c["reg"], c["srcbbox"], t, order, 2)
+
+
+# ---------------------------------------------------------------- higher-order restriction
+@needs_ref
+@pytest.mark.parametrize("order", [3, 5])
+def test_cc_higher_order_restriction_bit_exact_vs_reference(port, order):
+    """restrict_3d_cc_o3_rf2 / restrict_3d_cc_o5_rf2 (selected in CarpetLib by
+    use_higher_order_restriction and restriction_order_space) against the
+    reference's own operators, bit for bit in the canonical order, and the
+    fused order within the forward-error bound."""
+    ref = Ref(False)
+    rng = np.random.default_rng(500 + order)
+    reach = (1, 1) if order == 3 else (2, 2)
+    for it in range(25):
+        c = cases.cc_restrict_case(rng, half=int(rng.choice([1, 2])), max_ext=8, kind="mixed",
+                                   reach=reach)
+        d1, d2, d3 = c["dst"].copy(), c["dst"].copy(), c["dst"].copy()
+        port.restrict_3d_cc_ho_rf2(order, c["src"], c["srcbbox"], d1, c["dstbbox"], c["reg"])
+        ref.restrict_3d_cc_ho_rf2(order, c["src"], c["srcbbox"], d2, c["dstbbox"], c["reg"])
+        assert bits_equal(d1, d2)
+        port.restrict_3d_cc_ho_rf2(order, c["src"], c["srcbbox"], d3, c["dstbbox"], c["reg"], fma=True)
+        r1 = cases.region_view(d1, c["dstbbox"], c["reg"])
+        r3 = cases.region_view(d3, c["dstbbox"], c["reg"])
+        # |weights| sum to 1.25 (order 3) / 1.42 (order 5) per axis
+        assert np.abs(r1 - r3).max() <= 4 * np.finfo(float).eps * np.abs(c["src"]).max() * 1.6 ** 3
+
+
+def test_higher_order_restriction_selection(port):
+    """transfer's cell-centred restriction follows the parameters: order 1
+    (or the parameter off) is restrict_3d_cc_rf2, 3 and 5 the higher-order
+    stencils, anything else an error; ENO keeps the 8-point average"""
+    rng = np.random.default_rng(510)
+    c = cases.cc_restrict_case(rng, max_ext=6, reach=(2, 2))
+    outs = {}
+    try:
+        for use, order, op in ((False, 5, OP_LAGRANGE), (True, 1, OP_LAGRANGE), (True, 3, OP_LAGRANGE),
+                               (True, 5, OP_LAGRANGE), (True, 5, OP_ENO)):
+            port.set_restriction(use, order)
+            d = c["dst"].copy()
+            port.transfer(op, CELL, d, c["dstbbox"], [c["src"]], c["srcbbox"], [0.0], c["reg"],
+                          c["srcbbox"], 0.0, 0, 0)
+            outs[(use, order, op)] = d
+        port.set_restriction(True, 4)
+        with pytest.raises(OracleError):
+            port.transfer(OP_LAGRANGE, CELL, c["dst"].copy(), c["dstbbox"], [c["src"]], c["srcbbox"],
+                          [0.0], c["reg"], c["srcbbox"], 0.0, 0, 0)
+    finally:
+        port.set_restriction(False, 1)
+    avg = c["dst"].copy()
+    port.restrict_3d_cc_rf2(c["src"], c["srcbbox"], avg, c["dstbbox"], c["reg"])
+    for order in (3, 5):
+        d = c["dst"].copy()
+        port.restrict_3d_cc_ho_rf2(order, c["src"], c["srcbbox"], d, c["dstbbox"], c["reg"])
+        assert bits_equal(outs[(True, order, OP_LAGRANGE)], d)
+    for key in ((False, 5, OP_LAGRANGE), (True, 1, OP_LAGRANGE), (True, 5, OP_ENO)):
+        assert bits_equal(outs[key], avg)
