@@ -32,6 +32,8 @@ namespace {
 
 thread_local std::string g_err;
 int g_fp_mode = CGX_FP_EXACT;
+// use_higher_order_restriction / restriction_order_space (CarpetLib/param.ccl)
+int g_ho_restrict = 0, g_restrict_order = 1;
 
 int fail(int code, const char *fmt, ...) {
   char buf[512];
@@ -391,6 +393,40 @@ int build_spatial(int op, int cent, const cgx_array *dst, const cgx_array *src,
       out->points = reg.npoints();
       out->bytes = 16 * out->points;
     } else if (cent == CGX_CELL) {
+      // data.cc:1061-1097: the parameters pick the stencil, except for the
+      // ENO and WENO transport operators
+      int ho = 0;
+      if (g_ho_restrict && op != CGX_OP_ENO && op != CGX_OP_WENO) {
+        if (g_restrict_order == 3 || g_restrict_order == 5) ho = g_restrict_order;
+        else if (g_restrict_order != 1)
+          return fail(CGX_EINVAL, "There is no restriction stencil with restriction_order_space==%d",
+                      g_restrict_order);
+      }
+      if (ho) {
+        // restrict_3d_cc_o3_rf2.cc:33-144 / restrict_3d_cc_o5_rf2.cc:79-157:
+        // the fine cells 2i+lo .. 2i+hi (per axis) around every coarse point
+        // must lie inside the source
+        const char *who = ho == 3 ? "restrict_3d_cc_o3_rf2" : "restrict_3d_cc_o5_rf2";
+        const int lo = ho == 3 ? -1 : -2, hi = ho == 3 ? 2 : 3;
+        if (!reg.in(regdst)) return fail(CGX_EINVAL, "%s: region extent is not contained in array extent", who);
+        for (int k = 0; k < 3; ++k) {
+          int h = sb.str[k] / 2;
+          if (sb.str[k] % 2 || (reg.lo[k] - sb.lo[k] - h) % sb.str[k] ||
+              (reg.lo[k] - regdst.lo[k]) % regdst.str[k])
+            return fail(CGX_EINVAL, "%s: region not aligned", who);
+          d.n[k] = reg.size(k);
+          d.soff[k] = (reg.lo[k] - sb.lo[k] - h) / sb.str[k];
+          if (d.soff[k] + lo < 0 || d.soff[k] + 2 * (d.n[k] - 1) + hi >= sb.size(k))
+            return fail(CGX_EINVAL, "%s: stencil reaches outside the source array", who);
+        }
+        d.kind = ho == 3 ? K_RESTRICT_CC3 : K_RESTRICT_CC5;
+        out->points = reg.npoints();
+        // compulsory traffic: the 8 fine cells under each coarse point once
+        // (the wider stencils re-read neighbours from cache) and the write
+        out->bytes = 72 * out->points;
+        d.order = 0;
+        return CGX_OK;
+      }
       // bbox::expanded_for (bbox.cc:208-219) of the region onto the source
       Box ef = reg;
       for (int k = 0; k < 3; ++k) {
@@ -596,6 +632,12 @@ int cgx_init(int device, int fp_mode) {
 int cgx_set_fp_mode(int fp_mode) {
   if (fp_mode != CGX_FP_EXACT && fp_mode != CGX_FP_FMA) return fail(CGX_EINVAL, "bad fp mode");
   g_fp_mode = fp_mode;
+  return CGX_OK;
+}
+
+int cgx_set_restriction(int use_higher_order, int order) {
+  g_ho_restrict = use_higher_order != 0;
+  g_restrict_order = order;
   return CGX_OK;
 }
 

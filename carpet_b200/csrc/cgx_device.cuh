@@ -25,7 +25,9 @@ enum Kind : int {
   K_PROLONG_VC = 3,  // prolongate_3d_rf2<ORDER>
   K_PROLONG_CC = 4,  // prolongate_3d_cc_rf2<ORDER>
   K_PROLONG_ENO = 5, // prolongate_3d_real8_eno
-  K_NKINDS = 6
+  K_RESTRICT_CC3 = 6, // restrict_3d_cc_o3_rf2 (4x4x4 cells)
+  K_RESTRICT_CC5 = 7, // restrict_3d_cc_o5_rf2 (6x6x6 cells, separable)
+  K_NKINDS = 8
 };
 
 enum TKind : int { T_NONE = 0, T_LIN = 1, T_QUAD = 2, T_ENO = 3 };
@@ -250,12 +252,16 @@ enum StreamVariant : int {
   SV_COPY3E = 3,      // copy, ENO time interpolation
   SV_RESTRICT_VC = 4, // injection
   SV_RESTRICT_CC = 5, // 8-point average
-  SV_COUNT = 6
+  SV_RESTRICT_CC3 = 6, // third-order cell-centred restriction
+  SV_RESTRICT_CC5 = 7, // fifth-order cell-centred restriction
+  SV_COUNT = 8
 };
 
 template <class D> __host__ __device__ __forceinline__ int stream_variant(const D &d) {
   if (d.kind == K_RESTRICT_VC) return SV_RESTRICT_VC;
   if (d.kind == K_RESTRICT_CC) return SV_RESTRICT_CC;
+  if (d.kind == K_RESTRICT_CC3) return SV_RESTRICT_CC3;
+  if (d.kind == K_RESTRICT_CC5) return SV_RESTRICT_CC5;
   if (d.kind != K_COPY) return -1;
   if (d.ntl == 1) return SV_COPY1;
   if (d.ntl == 2) return SV_COPY2;
@@ -383,6 +389,84 @@ __device__ __forceinline__ void restrict_cc_tile(const D &d, int tile, int lid) 
     res = madd<FMA>(w, a6, res);
     res = madd<FMA>(w, a7, res);
     dst[i + j * d.dsy + k * d.dsz] = res;
+  }
+}
+
+// restrict_3d_cc_o3_rf2 (restrict_3d_cc_o3_rf2.cc:147-211): the 4x4x4 fine
+// cells 2i-1 .. 2i+2 per axis (from the region's first cell soff), weights
+// c_a c_b c_c / 4096 with c = (-1, 9, 9, -1), summed left to right, x
+// fastest; the first term is a plain product.
+template <int FMA, int LANES, class D>
+__device__ __forceinline__ void restrict_cc3_tile(const D &d, int tile, int lid) {
+  constexpr int PER = STILE / LANES;
+  const unsigned npts = (unsigned)d.n[0] * d.n[1] * d.n[2];
+  const unsigned p0 = (unsigned)tile * STILE + lid;
+  const long long ssy = d.ssy, ssz = d.ssz;
+  const double *s0 = d.src[0] + (d.soff[0] - 1 + (d.soff[1] - 1) * ssy + (d.soff[2] - 1) * ssz);
+  double *dst = d.dst + (d.doff[0] + d.doff[1] * d.dsy + d.doff[2] * d.dsz);
+#pragma unroll 1
+  for (int r = 0; r < PER; ++r) {
+    const unsigned p = p0 + r * LANES;
+    if (p >= npts) break;
+    int i, j, k;
+    unflatten(d, p, i, j, k);
+    const double *q = s0 + 2 * (i + j * ssy + k * ssz);
+    double res = 0.0;
+    // one plane of 16 cells per pass; every weight is an exact binary
+    // fraction, so forming it from the plane's factor loses nothing
+#pragma unroll 1
+    for (int c = 0; c < 4; ++c) {
+      const double cz = (c == 0 || c == 3) ? -1.0 : 9.0;
+      const double *qz = q + c * ssz;
+      static_for<16>([&](auto M) {
+        constexpr int m = decltype(M)::value;
+        constexpr double cx = (m & 3) == 0 || (m & 3) == 3 ? -1.0 : 9.0;
+        constexpr double cy = (m >> 2) == 0 || (m >> 2) == 3 ? -1.0 : 9.0;
+        const double w = cx * cy * cz / 4096.0;
+        const double v = __ldg(qz + (m & 3) + (m >> 2) * ssy);
+        res = (m == 0 && c == 0) ? mul(w, v) : madd<FMA>(w, v, res);
+      });
+    }
+    dst[i + j * d.dsy + k * d.dsz] = res;
+  }
+}
+
+// restrict_3d_cc_o5_rf2 (restrict_3d_cc_o5_rf2.cc:36-78): restrict3 over the
+// planes 2k-2 .. 2k+3 of restrict2 over rows of restrict1 over the cells
+// 2i-2 .. 2i+3, each a left-to-right sum with weights (3, -25, 150, 150,
+// -25, 3) / 256, the first term a plain product.
+template <int FMA, int LANES, class D>
+__device__ __forceinline__ void restrict_cc5_tile(const D &d, int tile, int lid) {
+  constexpr int PER = STILE / LANES;
+  const unsigned npts = (unsigned)d.n[0] * d.n[1] * d.n[2];
+  const unsigned p0 = (unsigned)tile * STILE + lid;
+  const long long ssy = d.ssy, ssz = d.ssz;
+  const double *s0 = d.src[0] + (d.soff[0] - 2 + (d.soff[1] - 2) * ssy + (d.soff[2] - 2) * ssz);
+  double *dst = d.dst + (d.doff[0] + d.doff[1] * d.dsy + d.doff[2] * d.dsz);
+  constexpr double w[6] = {3.0 / 256, -25.0 / 256, 150.0 / 256, 150.0 / 256, -25.0 / 256, 3.0 / 256};
+#pragma unroll 1
+  for (int r = 0; r < PER; ++r) {
+    const unsigned p = p0 + r * LANES;
+    if (p >= npts) break;
+    int i, j, k;
+    unflatten(d, p, i, j, k);
+    const double *q = s0 + 2 * (i + j * ssy + k * ssz);
+    double r3 = 0.0;
+#pragma unroll 1
+    for (int c = 0; c < 6; ++c) {
+      double r2 = 0.0;
+#pragma unroll
+      for (int b = 0; b < 6; ++b) {
+        const double *row = q + c * ssz + b * ssy;
+        double r1 = mul(w[0], __ldg(row));
+#pragma unroll
+        for (int a = 1; a < 6; ++a) r1 = madd<FMA>(w[a], __ldg(row + a), r1);
+        r2 = b == 0 ? mul(w[0], r1) : madd<FMA>(w[b], r1, r2);
+      }
+      const double wc = (c == 0 || c == 5) ? w[0] : (c == 1 || c == 4) ? w[1] : w[2];
+      r3 = c == 0 ? mul(wc, r2) : madd<FMA>(wc, r2, r3);
+    }
+    dst[i + j * d.dsy + k * d.dsz] = r3;
   }
 }
 

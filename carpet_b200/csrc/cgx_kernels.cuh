@@ -47,6 +47,12 @@ static __device__ __noinline__ void restrict_vc_entry(const Desc &d, int tile) {
 template <int FMA> __device__ __noinline__ void restrict_cc_entry(const Desc &d, int tile) {
   restrict_cc_tile<FMA, NTHREADS>(d, tile, threadIdx.x);
 }
+template <int FMA> __device__ __noinline__ void restrict_cc3_entry(const Desc &d, int tile) {
+  restrict_cc3_tile<FMA, NTHREADS>(d, tile, threadIdx.x);
+}
+template <int FMA> __device__ __noinline__ void restrict_cc5_entry(const Desc &d, int tile) {
+  restrict_cc5_tile<FMA, NTHREADS>(d, tile, threadIdx.x);
+}
 
 template <class F, int FMA>
 __device__ __forceinline__ void prolong_ntl(const Desc &d, int tile, double *sm) {
@@ -73,6 +79,8 @@ __device__ __forceinline__ void run_tile(const Desc &d, int tile, double *sm, in
     return;
   case K_RESTRICT_VC: restrict_vc_entry(d, tile); return;
   case K_RESTRICT_CC: restrict_cc_entry<FMA>(d, tile); return;
+  case K_RESTRICT_CC3: restrict_cc3_entry<FMA>(d, tile); return;
+  case K_RESTRICT_CC5: restrict_cc5_entry<FMA>(d, tile); return;
   case K_PROLONG_VC:
     if (HIGH) {
       switch (d.order) {
@@ -208,7 +216,9 @@ __device__ __forceinline__ void stream_tile(const Desc &d, int tile, int lid) {
   else if (V == SV_COPY3Q) copy_tile<FMA, 3, T_QUAD, LANES>(d, tile, lid);
   else if (V == SV_COPY3E) copy_tile<FMA, 3, T_ENO, LANES>(d, tile, lid);
   else if (V == SV_RESTRICT_VC) restrict_vc_tile<LANES>(d, tile, lid);
-  else restrict_cc_tile<FMA, LANES>(d, tile, lid);
+  else if (V == SV_RESTRICT_CC) restrict_cc_tile<FMA, LANES>(d, tile, lid);
+  else if (V == SV_RESTRICT_CC3) restrict_cc3_tile<FMA, LANES>(d, tile, lid);
+  else restrict_cc5_tile<FMA, LANES>(d, tile, lid);
 }
 
 // Per-box form: a CTA per tile, every variant in one dispatch.  The
@@ -228,6 +238,8 @@ __global__ void __launch_bounds__(NTHREADS, STREAM_BLOCKS_PER_SM)
   case SV_COPY3E: stream_tile<FMA, SV_COPY3E, NTHREADS>(s_d, t, l); return;
   case SV_RESTRICT_VC: stream_tile<FMA, SV_RESTRICT_VC, NTHREADS>(s_d, t, l); return;
   case SV_RESTRICT_CC: stream_tile<FMA, SV_RESTRICT_CC, NTHREADS>(s_d, t, l); return;
+  case SV_RESTRICT_CC3: stream_tile<FMA, SV_RESTRICT_CC3, NTHREADS>(s_d, t, l); return;
+  case SV_RESTRICT_CC5: stream_tile<FMA, SV_RESTRICT_CC5, NTHREADS>(s_d, t, l); return;
   }
   if (threadIdx.x == 0) report(status, CGX_EDEVICE);
 }

@@ -31,6 +31,14 @@ def set_fp_mode(fma: bool):
     check(lib.cgx_set_fp_mode(_lib.FP_FMA if fma else _lib.FP_EXACT))
 
 
+def set_restriction(use_higher_order: bool, order: int = 1):
+    """CarpetLib's use_higher_order_restriction / restriction_order_space
+    (CarpetLib/param.ccl, data.cc:1061-1097): cell-centred restriction then
+    uses the third- or fifth-order stencil; takes effect for transfers built
+    afterwards"""
+    check(lib.cgx_set_restriction(int(bool(use_higher_order)), int(order)))
+
+
 def box_sizes(b: Sequence[int]):
     return tuple(max(0, (b[3 + d] - b[d] + b[6 + d]) // b[6 + d]) for d in range(3))
 

@@ -69,6 +69,13 @@ typedef struct cgx_array {
 /* Library state: floating-point mode and the default device. */
 int cgx_init(int device, int fp_mode);
 int cgx_set_fp_mode(int fp_mode);
+/* CarpetLib's use_higher_order_restriction and restriction_order_space
+ * parameters (CarpetLib/param.ccl; data.cc:1061-1097): with the first set,
+ * cell-centred restriction of a non-ENO/WENO operator uses
+ * restrict_3d_cc_o3_rf2 (order 3) or restrict_3d_cc_o5_rf2 (order 5);
+ * order 1 keeps restrict_3d_cc_rf2, any other order makes such transfers
+ * fail with CGX_EINVAL.  Process-wide; default off. */
+int cgx_set_restriction(int use_higher_order, int order);
 const char *cgx_last_error(void);
 const char *cgx_version(void);
 

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from oracle import cases
-from oracle.binding import OP_COPY, OP_ENO, OP_LAGRANGE, CELL, VERTEX
+from oracle.binding import OP_COPY, OP_ENO, OP_LAGRANGE, CELL, VERTEX, OracleError, alloc
 
 pytestmark = pytest.mark.gpu
 
@@ -137,6 +137,44 @@ def test_restrict_and_copy(cgx, port, fma, form):
         for ntl in (1, 2, 3):
             got, want = run_pair(cgx, port, c, OP_LAGRANGE, VERTEX, 1, ntl, fma, rng, form)
             assert bits_equal(got, want)
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("fma", [False, True], ids=["exact", "fma"])
+@pytest.mark.parametrize("order", [3, 5])
+def test_cc_higher_order_restriction(cgx, port, order, fma, form):
+    """restrict_3d_cc_o3_rf2 / _o5_rf2, selected as CarpetLib selects them
+    (use_higher_order_restriction with restriction_order_space)."""
+    rng = np.random.default_rng(4200 + order)
+    reach = (1, 1) if order == 3 else (2, 2)
+    cgx.set_restriction(True, order)
+    port.set_restriction(True, order)
+    try:
+        for it in range(8):
+            c = cases.cc_restrict_case(rng, half=int(rng.choice([1, 2])), reach=reach,
+                                       max_ext=40 if it == 7 else 9,
+                                       kind=("normal", "mixed")[it % 2])
+            got, want = run_pair(cgx, port, c, OP_LAGRANGE, CELL, 1, 1, fma, rng, form)
+            assert bits_equal(got, want)
+        # the ENO transport operator keeps the 8-cell average
+        c = cases.cc_restrict_case(rng, reach=reach, kind="mixed")
+        got, want = run_pair(cgx, port, c, OP_ENO, CELL, 1, 1, fma, rng, form)
+        assert bits_equal(got, want)
+        # a source without the stencil's reach is refused, as by the oracle
+        c = cases.cc_restrict_case(rng, kind="mixed")
+        reg, fs = c["reg"], c["srcbbox"][6]
+        srcbbox = [reg[d] - fs // 2 for d in range(3)] + [reg[3 + d] + fs // 2 for d in range(3)] + [fs] * 3
+        src = alloc(srcbbox)
+        with pytest.raises(OracleError, match="stencil reaches outside"):
+            port.transfer(OP_LAGRANGE, CELL, c["dst"].copy(), c["dstbbox"], [src], srcbbox, [0.0], reg,
+                          srcbbox, 0.0, 1, 0, fma=fma)
+        cgx.set_fp_mode(fma)
+        with pytest.raises(cgx.CgxError, match="stencil reaches outside"):
+            cgx.transfer_data(to_dev(cgx, c["dst"], c["dstbbox"]), [to_dev(cgx, src, srcbbox)], [0.0],
+                              reg, srcbbox, 0.0, 1, 0, op=OP_LAGRANGE, cent=CELL)
+    finally:
+        cgx.set_restriction(False, 1)
+        port.set_restriction(False, 1)
 
 
 def test_copy_with_slab_offset(cgx, port):
