@@ -94,6 +94,10 @@ class Port:
         self._op(self.lib.cgxo_prolongate_3d_cc_rf2, (order, int(fma)), src,
                  srcbbox, dst, dstbbox, reg, reg)
 
+    def prolongate_3d_cc_eno_rf2(self, order, src, srcbbox, dst, dstbbox, reg, fma=False):
+        self._op(self.lib.cgxo_prolongate_3d_cc_eno_rf2, (order, int(fma)), src,
+                 srcbbox, dst, dstbbox, reg, reg)
+
     def prolongate_3d_eno(self, src, srcbbox, dst, dstbbox, reg, fma=False):
         self._op(self.lib.cgxo_prolongate_3d_eno, (int(fma),), src, srcbbox, dst,
                  dstbbox, reg, reg)
@@ -203,6 +207,10 @@ class Ref:
 
     def prolongate_3d_cc_rf2(self, order, src, srcbbox, dst, dstbbox, reg):
         self._op(self.lib.cgxref_prolongate_3d_cc_rf2, (order,), src, srcbbox, dst,
+                 dstbbox, reg, reg)
+
+    def prolongate_3d_cc_eno_rf2(self, order, src, srcbbox, dst, dstbbox, reg):
+        self._op(self.lib.cgxref_prolongate_3d_cc_eno_rf2, (order,), src, srcbbox, dst,
                  dstbbox, reg, reg)
 
     def restrict_3d_rf2(self, src, srcbbox, dst, dstbbox, reg):

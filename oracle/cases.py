@@ -36,6 +36,14 @@ def _fill(rng, a, kind="normal"):
         # piecewise-constant with jumps: exercises the ENO limiters
         a[...] = np.sign(rng.standard_normal(a.shape)) * rng.integers(
             0, 3, a.shape).astype(np.float64)
+    elif kind == "smooth":
+        # smooth fields whose undivided differences keep their sign over
+        # stretches and change it elsewhere: every ENO stencil choice occurs
+        z, y, x = np.meshgrid(*[np.arange(n, dtype=np.float64) for n in a.shape], indexing="ij")
+        g = rng.uniform(-0.5, 0.5, 3)
+        f = rng.uniform(0.1, 0.9, 3)
+        a[...] = np.exp(g[0] * x + g[1] * y + g[2] * z) + 0.3 * np.sin(
+            f[0] * x + f[1] * y + f[2] * z + rng.uniform(0, 6.3))
     else:
         raise ValueError(kind)
     return a

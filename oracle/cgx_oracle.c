@@ -515,6 +515,146 @@ int cgxo_prolongate_3d_eno(int fma_, const double *src, const int *srcpadext,
 }
 
 /* ------------------------------------------------------------------ */
+/* prolongate_3d_cc_eno_rf2, CarpetLib/src/prolongate_3d_cc_eno_rf2.cc  */
+/* (ORDER 2 and 3; data.cc:689-720 maps order_space 2-4 to 2, 5 to 3)  */
+
+/* coeffs1dc<RT,ORDER,OFFSET> (:144-176), exact dyadic rationals */
+static const double ceno_first[2] = {1 / 4.0, 3 / 4.0};                 /* <1,0> */
+static const double ceno2_0[3] = {5 / 32.0, 30 / 32.0, -3 / 32.0};      /* <2,0> */
+static const double ceno2_m[3] = {-3 / 32.0, 14 / 32.0, 21 / 32.0};     /* <2,-1> */
+static const double ceno3_0[4] = {-5 / 128.0, 35 / 128.0, 105 / 128.0, -7 / 128.0};
+static const double ceno3_p[4] = {15 / 128.0, 135 / 128.0, -27 / 128.0, 5 / 128.0};
+static const double ceno3_m[4] = {7 / 128.0, -33 / 128.0, 77 / 128.0, 77 / 128.0};
+
+/* coeffs1d<>::get (:73-85): res = 0; res += get(i) * f(i) for i from imin,
+ * the table reversed for the odd parity; p points at the coarse base */
+static double ceno_sum(int fma_, const double *tab, int n, int imin, int di, const double *p) {
+  double r = 0.0;
+  for (int i = imin; i < imin + n; ++i) {
+    int j = di == 0 ? i - imin : n - 1 - (i - imin);
+    r = madd(fma_, tab[j], p[i], r);
+  }
+  return r;
+}
+/* the undivided differences, diffC1dc (:171-174) applied with coeffs1d::diff
+ * (:87-96, never reversed) */
+static double ceno_diff(int fma_, int order, int imin, const double *p) {
+  static const double d2[3] = {1, -2, 1}, d3[4] = {1, -3, 3, -1};
+  const double *d = order == 2 ? d2 : d3;
+  double r = 0.0;
+  for (int i = imin; i < imin + order + 1; ++i) r = madd(fma_, d[i - imin], p[i], r);
+  return r;
+}
+/* one axis of interp1/interp2/interp3 (:198-371, the three are the same
+ * rule): the smoothest of the shifted stencils, first order where the
+ * differences change sign or the result leaves [f(di-1), f(di)].  The
+ * window is f(-2+di) .. f(1+di) for ORDER 2 and f(-3+di) .. f(2+di) for 3. */
+static double ceno1d(int fma_, int order, int di, const double *p) {
+  double res;
+  if (order == 2) {
+    const int shift = di == 0 ? -1 : 1; /* :225-231 */
+    double lV = ceno_diff(fma_, 2, -1 + shift, p);
+    double rV = ceno_diff(fma_, 2, -1, p);
+    if (lV * rV <= 0)
+      res = ceno_sum(fma_, ceno_first, 2, -1 + di, di, p);
+    else if (fabs(lV) < fabs(rV))
+      res = ceno_sum(fma_, ceno2_m, 3, -1 + shift, di, p);
+    else
+      res = ceno_sum(fma_, ceno2_0, 3, -1, di, p);
+  } else {
+    /* shifts -1, 0, +1 (:289-306); coeffs1dc<3, di == 0 ? OFFSET : -OFFSET> */
+    const double *tl = di == 0 ? ceno3_m : ceno3_p, *tr = di == 0 ? ceno3_p : ceno3_m;
+    double V[3];
+    V[0] = ceno_diff(fma_, 3, -3 + di, p);
+    V[1] = ceno_diff(fma_, 3, -2 + di, p);
+    V[2] = ceno_diff(fma_, 3, -1 + di, p);
+    if (V[0] * V[2] <= 0 || V[0] * V[1] <= 0 || V[1] * V[2] <= 0)
+      return ceno_sum(fma_, ceno_first, 2, -1 + di, di, p); /* :311-329 */
+    int min = 1;
+    for (int i = 0; i < 3; ++i)
+      if (fabs(V[i]) < fabs(V[min])) min = i;
+    if (min == 0) res = ceno_sum(fma_, tl, 4, -3 + di, di, p);
+    else if (min == 1) res = ceno_sum(fma_, ceno3_0, 4, -2 + di, di, p);
+    else res = ceno_sum(fma_, tr, 4, -1 + di, di, p);
+  }
+  /* :366-395 */
+  if ((res - p[di - 1]) * (p[di] - res) < 0)
+    res = ceno_sum(fma_, ceno_first, 2, -1 + di, di, p);
+  return res;
+}
+
+int cgxo_prolongate_3d_cc_eno_rf2(int order, int fma_, const double *src,
+                                  const int *srcpadext, const int *srcext,
+                                  double *dst, const int *dstpadext,
+                                  const int *dstext, const int *srcbbox_,
+                                  const int *dstbbox_, const int *srcregbbox_,
+                                  const int *regbbox_) {
+  (void)srcregbbox_; (void)dstext;
+  if (order != 2 && order != 3)
+    return fail(CGXO_EUNSUPPORTED, "prolongate_3d_cc_eno_rf2: no stencil of order %d", order);
+  box_t srcbbox = mkbox(srcbbox_), dstbbox = mkbox(dstbbox_), reg = mkbox(regbbox_);
+  /* :962-981 */
+  for (int d = 0; d < 3; ++d) {
+    if (srcbbox.str[d] <= reg.str[d] || dstbbox.str[d] != reg.str[d])
+      return fail(CGXO_EINVAL, "prolongate_3d_cc_eno_rf2: strides disagree");
+    if (srcbbox.str[d] != 2 * dstbbox.str[d])
+      return fail(CGXO_EINVAL, "prolongate_3d_cc_eno_rf2: source strides are not twice the destination strides");
+    if (dstbbox.str[d] % 2 != 0)
+      return fail(CGXO_EINVAL, "prolongate_3d_cc_eno_rf2: destination strides are not even");
+  }
+  if (box_empty(&reg))
+    return fail(CGXO_EINVAL, "prolongate_3d_cc_eno_rf2: region extent is empty");
+  /* :983-1031: window of the parity at each end, in fine strides */
+  const int mm = order == 2 ? -2 : -3; /* coeffs1d<ORDER,di>::minimin - di */
+  int regext[3], srcoff[3], dstoff[3], offlo[3], offhi[3];
+  for (int d = 0; d < 3; ++d) {
+    regext[d] = box_size(&reg, d);
+    int h = reg.str[d] / 2;
+    if ((reg.lo[d] - srcbbox.lo[d] + h) % reg.str[d] ||
+        (reg.lo[d] - dstbbox.lo[d]) % reg.str[d] ||
+        (reg.up[d] - srcbbox.lo[d] + h) % reg.str[d])
+      return fail(CGXO_EINVAL, "prolongate_3d_cc_eno_rf2: region not aligned");
+    srcoff[d] = (reg.lo[d] - srcbbox.lo[d] + h) / reg.str[d];
+    dstoff[d] = (reg.lo[d] - dstbbox.lo[d]) / reg.str[d];
+    int srcend = (reg.up[d] - srcbbox.lo[d] + h) / reg.str[d];
+    offlo[d] = -(mm + srcoff[d] % 2);
+    offhi[d] = -mm + srcend % 2 - 1;
+  }
+  box_t ex = box_expand(&reg, offlo, offhi);
+  if (!box_in(&ex, &srcbbox) || !box_in(&reg, &dstbbox))
+    return fail(CGXO_EINVAL, "prolongate_3d_cc_eno_rf2: region extent is not contained in array extent");
+  /* that test counts fine strides; the coarse points actually read must be
+   * inside the source too (the reference only asserts it, :905-941) */
+  for (int d = 0; d < 3; ++d) {
+    /* fine point s reads coarse ceil(s/2) + mm .. ceil(s/2) - mm - 1 */
+    int s0 = srcoff[d], s1 = srcoff[d] + regext[d] - 1;
+    int lo = (s0 + 1) / 2 + mm, hi = (s1 + 1) / 2 - mm - 1;
+    if (lo < 0 || hi >= srcext[d])
+      return fail(CGXO_EINVAL, "prolongate_3d_cc_eno_rf2: stencil reaches outside the source array");
+  }
+  const int W = order == 2 ? 2 : 3; /* window f(-W+di) .. f(W-1+di) */
+  double xb[8], yb[8];
+  for (int k = 0; k < regext[2]; ++k) {
+    int sk = srcoff[2] + k, dk = sk & 1, ks = sk >> 1;
+    for (int j = 0; j < regext[1]; ++j) {
+      int sj = srcoff[1] + j, dj = sj & 1, js = sj >> 1;
+      for (int i = 0; i < regext[0]; ++i) {
+        int si = srcoff[0] + i, di = si & 1, is = si >> 1;
+        /* interp3 over interp2 over interp1 (:722-760) */
+        for (int kk = -W + dk; kk < W + dk; ++kk) {
+          for (int jj = -W + dj; jj < W + dj; ++jj)
+            xb[4 + jj] = ceno1d(fma_, order, di, &src[IDX(is, js + jj, ks + kk, srcpadext)]);
+          yb[4 + kk] = ceno1d(fma_, order, dj, &xb[4]);
+        }
+        dst[IDX(dstoff[0] + i, dstoff[1] + j, dstoff[2] + k, dstpadext)] =
+            ceno1d(fma_, order, dk, &yb[4]);
+      }
+    }
+  }
+  return CGXO_OK;
+}
+
+/* ------------------------------------------------------------------ */
 /* restrict_3d_rf2, CarpetLib/src/restrict_3d_rf2.cc:25-121             */
 
 int cgxo_restrict_3d_rf2(const double *src, const int *srcpadext,
@@ -944,6 +1084,15 @@ static int transfer_p_r(int fma_, int op, int cent, double *dst,
         return cgxo_prolongate_3d_eno(fma_, src, srcpadext, srcext, dst, dstpadext,
                                       dstext, srcbbox, dstbbox, srcbox, dstbox);
       return fail(CGXO_EINVAL, "transfer_prolongate: no ENO stencil for this order");
+    }
+    if (op == op_ENO && cent == cell_centered) {
+      /* data.cc:689-720: orders 2-4 run the second-order stencil, 5 the third */
+      if (order_space < 2 || order_space > 5)
+        return fail(CGXO_EINVAL, "There is no cell-centred stencil for op=\"ENO\" with "
+                                 "order_space not in {2,3,4,5}");
+      return cgxo_prolongate_3d_cc_eno_rf2(order_space == 5 ? 3 : 2, fma_, src, srcpadext,
+                                           srcext, dst, dstpadext, dstext, srcbbox, dstbbox,
+                                           srcbox, dstbox);
     }
     return fail(CGXO_EUNSUPPORTED, "transfer_prolongate: operator outside the restated set");
   }

@@ -145,6 +145,20 @@ int cgxref_prolongate_3d_cc_rf2(int order, OPARGS) {
   });
 }
 
+// prolongate_3d_cc_eno_rf2<double,ORDER>
+// (CarpetLib/src/prolongate_3d_cc_eno_rf2.cc:944), ORDER 2 or 3
+int cgxref_prolongate_3d_cc_eno_rf2(int order, OPARGS) {
+  return guarded([&] {
+    op_t op = nullptr;
+    switch (order) {
+    case 2: op = &prolongate_3d_cc_eno_rf2<double, 2>; break;
+    case 3: op = &prolongate_3d_cc_eno_rf2<double, 3>; break;
+    default: throw std::runtime_error("no cell-centred ENO stencil of this order");
+    }
+    call_operator(op, OPCALL);
+  });
+}
+
 // restrict_3d_rf2 (CarpetLib/src/restrict_3d_rf2.cc:25); called directly,
 // as CarpetLib/src/data.cc:1041 does through call_operator.
 int cgxref_restrict_3d_rf2(OPARGS) {

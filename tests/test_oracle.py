@@ -70,6 +70,54 @@ def test_cc_lagrange_bit_exact_vs_reference(port, order):
 
 
 @needs_ref
+@pytest.mark.parametrize("order", [2, 3])
+def test_cc_eno_bit_exact_vs_reference(port, order):
+    """prolongate_3d_cc_eno_rf2<ORDER>: the restatement against the compiled
+    reference, on data that drive every stencil choice and limiter branch"""
+    ref = Ref(False)
+    rng = np.random.default_rng(250 + order)
+    for it in range(36):
+        kind = ("normal", "mixed", "steps", "smooth")[it % 4]
+        # the Lagrange case of the same window: ORDER 2 reads as CC<3>, 3 as CC<5>
+        c = cases.cc_prolong_case(rng, 2 * order - 1, half=int(rng.choice([1, 2])), kind=kind)
+        d1, d2 = c["dst"].copy(), c["dst"].copy()
+        port.prolongate_3d_cc_eno_rf2(order, c["src"], c["srcbbox"], d1, c["dstbbox"], c["reg"])
+        ref.prolongate_3d_cc_eno_rf2(order, c["src"], c["srcbbox"], d2, c["dstbbox"], c["reg"])
+        assert bits_equal(d1, d2), (it, kind)
+
+
+def test_cc_eno_limiter_branches(port):
+    """The smooth fields reach the high-order stencils: the result differs
+    from the first-order fallback somewhere, and is exact for data that the
+    chosen stencils reproduce (a linear field stays linear)."""
+    rng = np.random.default_rng(260)
+    for order in (2, 3):
+        c = cases.cc_prolong_case(rng, 2 * order - 1, kind="smooth", max_ext=12)
+        d = c["dst"].copy()
+        port.prolongate_3d_cc_eno_rf2(order, c["src"], c["srcbbox"], d, c["dstbbox"], c["reg"])
+        # the first-order rule on every axis is prolongate_3d_cc_rf2<1>
+        d1 = c["dst"].copy()
+        port.prolongate_3d_cc_rf2(1, c["src"], c["srcbbox"], d1, c["dstbbox"], c["reg"])
+        assert not bits_equal(d, d1)
+        # a linear field: every undivided difference is zero, so the
+        # first-order rule runs; it interpolates linear data exactly
+        src = c["src"].copy()
+        lo, st = c["srcbbox"][:3], c["srcbbox"][6:9]
+        z, y, x = np.meshgrid(*[np.arange(n, dtype=np.float64) for n in src.shape], indexing="ij")
+        src[...] = (lo[0] + x * st[0]) + 2 * (lo[1] + y * st[1]) - 0.5 * (lo[2] + z * st[2])
+        d = c["dst"].copy()
+        port.prolongate_3d_cc_eno_rf2(order, src, c["srcbbox"], d, c["dstbbox"], c["reg"])
+        reg = c["reg"]
+        dlo, dst_ = c["dstbbox"][:3], c["dstbbox"][6:9]
+        n = box_sizes(reg)
+        o = [(reg[k] - dlo[k]) // dst_[k] for k in range(3)]
+        got = d[o[2]:o[2] + n[2], o[1]:o[1] + n[1], o[0]:o[0] + n[0]]
+        zz, yy, xx = np.meshgrid(*[reg[k] + np.arange(n[k]) * reg[6 + k] for k in (2, 1, 0)],
+                                 indexing="ij")
+        np.testing.assert_allclose(got, xx + 2 * yy - 0.5 * zz, rtol=0, atol=1e-9)
+
+
+@needs_ref
 def test_restrict_copy_time_bit_exact_vs_reference(port):
     ref = Ref(False)
     rng = np.random.default_rng(300)
@@ -332,3 +380,24 @@ def test_higher_order_restriction_selection(port):
         assert bits_equal(outs[(True, order, OP_LAGRANGE)], d)
     for key in ((False, 5, OP_LAGRANGE), (True, 1, OP_LAGRANGE), (True, 5, OP_ENO)):
         assert bits_equal(outs[key], avg)
+
+
+def test_cc_eno_order_selection(port):
+    """transfer's cell-centred ENO prolongation (data.cc:689-720): orders 2-4
+    run the second-order stencil, 5 the third, anything else an error"""
+    rng = np.random.default_rng(520)
+    c = cases.cc_prolong_case(rng, 5, max_ext=6, kind="smooth")
+    want = {}
+    for order in (2, 3):
+        d = c["dst"].copy()
+        port.prolongate_3d_cc_eno_rf2(order, c["src"], c["srcbbox"], d, c["dstbbox"], c["reg"])
+        want[order] = d
+    for order_space in (2, 3, 4, 5):
+        d = c["dst"].copy()
+        port.transfer(OP_ENO, CELL, d, c["dstbbox"], [c["src"]], c["srcbbox"], [0.0], c["reg"],
+                      c["srcbbox"], 0.0, order_space, 0)
+        assert bits_equal(d, want[3 if order_space == 5 else 2])
+    for order_space in (1, 6):
+        with pytest.raises(OracleError, match="order_space not in"):
+            port.transfer(OP_ENO, CELL, c["dst"].copy(), c["dstbbox"], [c["src"]], c["srcbbox"],
+                          [0.0], c["reg"], c["srcbbox"], 0.0, order_space, 0)
