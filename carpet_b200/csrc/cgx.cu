@@ -94,6 +94,7 @@ Win family_window(int kind, int order) {
     int n = order + 1, lo0 = -n / 2, lo1 = -n / 2 + (order % 2 ? 1 : 0);
     return {lo0, lo0 + n - 1, lo1, lo1 + n - 1};
   }
+  if (kind == K_PROLONG_CC_ENO) return {-order, order - 1, -order + 1, order};
   return {0, 0, -1, 2}; // ENO
 }
 
@@ -130,7 +131,7 @@ long long prolong_tiles(Desc &d, int pycmax, int pz) {
 // consecutive points of the flattened region.
 int kind_tiles(Desc &d) {
   const int kind = d.kind;
-  const bool prol = kind == K_PROLONG_VC || kind == K_PROLONG_CC || kind == K_PROLONG_ENO;
+  const bool prol = is_stencil(kind);
   long long tot = 1;
   if (prol) {
     tot = prolong_tiles(d, PTYCMAX, PTZ);
@@ -305,25 +306,33 @@ int build_spatial(int op, int cent, const cgx_array *dst, const cgx_array *src,
                       order_space);
         kind = K_PROLONG_CC;
       } else return fail(CGX_EINVAL, "transfer_prolongate: bad centering");
+    } else if (op == CGX_OP_ENO && cent == CGX_CELL) {
+      // data.cc:689-720: orders 2-4 run the second-order stencil, 5 the third
+      if (order_space < 2 || order_space > 5)
+        return fail(CGX_EINVAL, "There is no cell-centred stencil for op=\"ENO\" with "
+                                "order_space not in {2,3,4,5}");
+      kind = K_PROLONG_CC_ENO;
+      order_space = order_space == 5 ? 3 : 2;
     } else if (op == CGX_OP_ENO) {
-      if (cent != CGX_VERTEX)
-        return fail(CGX_EUNSUPPORTED, "transfer_prolongate: cell-centred ENO is not provided");
+      if (cent != CGX_VERTEX) return fail(CGX_EINVAL, "transfer_prolongate: bad centering");
       if (order_space != 3 && order_space != 5) // data.cc:660-686
         return fail(CGX_EINVAL, "transfer_prolongate: no ENO stencil of order %d", order_space);
       kind = K_PROLONG_ENO;
     } else return fail(CGX_EUNSUPPORTED, "transfer_prolongate: operator %d is not provided", op);
 
     // argument checks of prolongate_3d_rf2.cc:373-417,
-    // prolongate_3d_cc_rf2.cc:253-321, prolongate_3d_real8_eno.F90:122-175
+    // prolongate_3d_cc_rf2.cc:253-321, prolongate_3d_real8_eno.F90:122-175,
+    // prolongate_3d_cc_eno_rf2.cc:962-1031
+    const bool cellk = kind == K_PROLONG_CC || kind == K_PROLONG_CC_ENO;
     for (int k = 0; k < 3; ++k) {
       if (sb.str[k] <= reg.str[k] || regdst.str[k] != reg.str[k])
         return fail(CGX_EINVAL, "prolongate: strides disagree");
       if (sb.str[k] != 2 * regdst.str[k])
         return fail(CGX_EINVAL, "prolongate: source strides are not twice the destination strides");
-      if (kind != K_PROLONG_CC &&
+      if (!cellk &&
           (sb.lo[k] % sb.str[k] || regdst.lo[k] % regdst.str[k] || reg.lo[k] % reg.str[k]))
         return fail(CGX_EINVAL, "prolongate: bbox is not aligned with vertices");
-      if (kind == K_PROLONG_CC && regdst.str[k] % 2)
+      if (cellk && regdst.str[k] % 2)
         return fail(CGX_EINVAL, "prolongate_3d_cc_rf2: destination strides are not even");
     }
     if (reg.empty()) return fail(CGX_EINVAL, "prolongate: region extent is empty");
@@ -331,7 +340,7 @@ int build_spatial(int op, int cent, const cgx_array *dst, const cgx_array *src,
     const Win w = family_window(kind, order_space);
     long long ncoarse = 1;
     for (int k = 0; k < 3; ++k) {
-      const int h = kind == K_PROLONG_CC ? reg.str[k] / 2 : 0;
+      const int h = cellk ? reg.str[k] / 2 : 0;
       if ((reg.lo[k] - sb.lo[k] + h) % reg.str[k] || (reg.lo[k] - regdst.lo[k]) % reg.str[k])
         return fail(CGX_EINVAL, "prolongate: region not aligned with the arrays");
       d.n[k] = reg.size(k);
@@ -356,6 +365,17 @@ int build_spatial(int op, int cent, const cgx_array *dst, const cgx_array *src,
         ex.up[k] += ohi * reg.str[k];
       }
       if (!ex.in(sb)) return fail(CGX_EINVAL, "prolongate_3d_rf2: region extent is not contained in array extent");
+    } else if (kind == K_PROLONG_CC_ENO) {
+      // prolongate_3d_cc_eno_rf2.cc:994-1031: the window of the parity at
+      // each end, counted in fine strides
+      Box ex = reg;
+      for (int k = 0; k < 3; ++k) {
+        const int send = d.soff[k] + reg.size(k) - 1;
+        ex.lo[k] -= (order_space - d.soff[k] % 2) * reg.str[k];
+        ex.up[k] += (order_space + send % 2 - 1) * reg.str[k];
+      }
+      if (!ex.in(sb))
+        return fail(CGX_EINVAL, "prolongate_3d_cc_eno_rf2: region extent is not contained in array extent");
     }
     d.kind = kind;
     d.order = order_space;
@@ -1162,7 +1182,7 @@ int launch_tile_map(const Desc *d_descs, const CUtensorMap *d_maps, const int2 *
 }
 
 bool encode_tma_maps(const Desc &d, CUtensorMap maps[3]) {
-  if (!is_stencil(d.kind) || d.bx == 0 || (d.kind == K_PROLONG_VC && d.order >= 7)) return false;
+  if (!is_stencil(d.kind) || d.bx == 0 || tma_variant(d) < 0) return false;
   // row and plane pitches must be multiples of 16 bytes
   if (d.ssy % 2 || d.ssz % 2 || d.ssz >= (1LL << 37)) return false;
   PFN_cuTensorMapEncodeTiled_v12000 enc = tma_encoder();

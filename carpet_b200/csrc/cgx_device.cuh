@@ -27,7 +27,8 @@ enum Kind : int {
   K_PROLONG_ENO = 5, // prolongate_3d_real8_eno
   K_RESTRICT_CC3 = 6, // restrict_3d_cc_o3_rf2 (4x4x4 cells)
   K_RESTRICT_CC5 = 7, // restrict_3d_cc_o5_rf2 (6x6x6 cells, separable)
-  K_NKINDS = 8
+  K_PROLONG_CC_ENO = 8, // prolongate_3d_cc_eno_rf2<ORDER>, ORDER (d.order) 2 or 3
+  K_NKINDS = 9
 };
 
 enum TKind : int { T_NONE = 0, T_LIN = 1, T_QUAD = 2, T_ENO = 3 };
@@ -190,6 +191,77 @@ struct ENO {
   template <int FMA, class G> __device__ __forceinline__ static double next(int par, G get) {
     if (!par) return get(0);
     return eno1d<FMA>(get(-1), get(0), get(1), get(2));
+  }
+  template <int FMA, class G> __device__ __forceinline__ static double first(int par, G get) {
+    return next<FMA>(par, get);
+  }
+};
+
+// cell-centred ENO, prolongate_3d_cc_eno_rf2.cc:198-400 (interp1, interp2
+// and interp3 apply the same rule on their axis).  Relative to the coarse
+// base c, the fine point of parity DI reads f(-W+DI) .. f(W-1+DI), W = ORDER.
+// coeffs1dc<RT,ORDER,OFFSET> (:144-176) as exact dyadic rationals; table t:
+// 0 <1,0>, 1 <2,0>, 2 <2,-1>, 3 <3,0>, 4 <3,+1>, 5 <3,-1>.
+__device__ __forceinline__ constexpr double ceno_coeff(int t, int j) {
+  return t == 0 ? (j == 0 ? 1.0 : 3.0) / 4
+       : t == 1 ? (j == 0 ? 5.0 : j == 1 ? 30.0 : -3.0) / 32
+       : t == 2 ? (j == 0 ? -3.0 : j == 1 ? 14.0 : 21.0) / 32
+       : t == 3 ? (j == 0 ? -5.0 : j == 1 ? 35.0 : j == 2 ? 105.0 : -7.0) / 128
+       : t == 4 ? (j == 0 ? 15.0 : j == 1 ? 135.0 : j == 2 ? -27.0 : 5.0) / 128
+                : (j == 0 ? 7.0 : j == 1 ? -33.0 : 77.0) / 128;
+}
+template <int ORDER> struct CCENO {
+  static_assert(ORDER == 2 || ORDER == 3, "cell-centred ENO orders 2 and 3");
+  static constexpr int LO = -ORDER, HI = ORDER;
+  // coeffs1d::get summed from imin: res = 0; res += c*f (reversed for DI=1)
+  template <int FMA, int DI, int T, int N, int IMIN, class G>
+  __device__ __forceinline__ static double sum(G get) {
+    double r = 0.0;
+    static_for<N>([&](auto M) {
+      constexpr int m = decltype(M)::value;
+      r = madd<FMA>(ceno_coeff(T, DI == 0 ? m : N - 1 - m), get(IMIN + m), r);
+    });
+    return r;
+  }
+  // undivided differences (diffC1dc, :171-174; never reversed)
+  template <int FMA, int IMIN, class G> __device__ __forceinline__ static double diff(G get) {
+    double r = 0.0;
+    static_for<ORDER + 1>([&](auto M) {
+      constexpr int m = decltype(M)::value;
+      constexpr double c = ORDER == 2 ? (m == 1 ? -2.0 : 1.0)
+                                      : (m == 0 ? 1.0 : m == 1 ? -3.0 : m == 2 ? 3.0 : -1.0);
+      r = madd<FMA>(c, get(IMIN + m), r);
+    });
+    return r;
+  }
+  template <int FMA, int DI, class G> __device__ __forceinline__ static double rule(G get) {
+    const double first = sum<FMA, DI, 0, 2, -1 + DI>(get); // coeffs1d<RT,1,di,0>
+    double res;
+    if (ORDER == 2) {
+      constexpr int SH = DI == 0 ? -1 : 1; // :225-231
+      const double lV = diff<FMA, -1 + SH>(get), rV = diff<FMA, -1>(get);
+      if (__dmul_rn(lV, rV) <= 0.0) res = first;
+      else if (fabs(lV) < fabs(rV)) res = sum<FMA, DI, 2, 3, -1 + SH>(get);
+      else res = sum<FMA, DI, 1, 3, -1>(get);
+    } else {
+      const double V0 = diff<FMA, -3 + DI>(get), V1 = diff<FMA, -2 + DI>(get),
+                   V2 = diff<FMA, -1 + DI>(get);
+      if (__dmul_rn(V0, V2) <= 0.0 || __dmul_rn(V0, V1) <= 0.0 || __dmul_rn(V1, V2) <= 0.0)
+        return first; // :311-329, without the final test
+      int mn = 1;
+      if (fabs(V0) < fabs(V1)) mn = 0;
+      if (fabs(V2) < fabs(mn == 0 ? V0 : V1)) mn = 2;
+      // coeffs1dc<3, di == 0 ? OFFSET : -OFFSET> for OFFSET -1, 0, +1
+      if (mn == 0) res = sum<FMA, DI, DI == 0 ? 5 : 4, 4, -3 + DI>(get);
+      else if (mn == 1) res = sum<FMA, DI, 3, 4, -2 + DI>(get);
+      else res = sum<FMA, DI, DI == 0 ? 4 : 5, 4, -1 + DI>(get);
+    }
+    // :366-395: a result outside the two nearest values falls back
+    if (__dmul_rn(__dsub_rn(res, get(DI - 1)), __dsub_rn(get(DI), res)) < 0.0) res = first;
+    return res;
+  }
+  template <int FMA, class G> __device__ __forceinline__ static double next(int par, G get) {
+    return par ? rule<FMA, 1>(get) : rule<FMA, 0>(get);
   }
   template <int FMA, class G> __device__ __forceinline__ static double first(int par, G get) {
     return next<FMA>(par, get);

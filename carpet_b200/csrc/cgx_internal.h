@@ -88,7 +88,8 @@ int klaunch_stream_f1(int variant, const Desc *d, const int2 *tmap, long long nt
 // stencil (prolongation) kinds run in the shared-memory kernels, the others
 // in the streaming kernels
 inline bool is_stencil(int kind) {
-  return kind == K_PROLONG_VC || kind == K_PROLONG_CC || kind == K_PROLONG_ENO;
+  return kind == K_PROLONG_VC || kind == K_PROLONG_CC || kind == K_PROLONG_ENO ||
+         kind == K_PROLONG_CC_ENO;
 }
 inline int segment_of(const Desc &d) {
   if (!is_stencil(d.kind)) return SEG_STREAM + stream_variant(d);

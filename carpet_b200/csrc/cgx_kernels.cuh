@@ -96,6 +96,12 @@ __device__ __forceinline__ void run_tile(const Desc &d, int tile, double *sm, in
       }
     }
     break;
+  case K_PROLONG_CC_ENO:
+    if (!HIGH) {
+      if (d.order == 2) { prolong_ntl<CCENO<2>, FMA>(d, tile, sm); return; }
+      if (d.order == 3) { prolong_ntl<CCENO<3>, FMA>(d, tile, sm); return; }
+    }
+    break;
   case K_PROLONG_CC:
     if (!HIGH) {
       switch (d.order) {

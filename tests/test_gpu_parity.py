@@ -125,6 +125,23 @@ def test_vc_eno(cgx, port, ntl, fma, form):
 
 @pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("fma", [False, True], ids=["exact", "fma"])
+@pytest.mark.parametrize("ntl", [1, 2, 3])
+@pytest.mark.parametrize("order_space", [2, 3, 4, 5])
+def test_cc_eno(cgx, port, order_space, ntl, fma, form):
+    """prolongate_3d_cc_eno_rf2 (order_space 2-4: ORDER 2, 5: ORDER 3) with
+    ENO time interpolation, on data that drive every stencil choice"""
+    rng = np.random.default_rng(3100 + 10 * order_space + ntl)
+    lagr = 5 if order_space == 5 else 3  # the Lagrange order of the same window
+    for it in range(8):
+        c = cases.cc_prolong_case(rng, lagr, half=int(rng.choice([1, 2])),
+                                  max_ext=36 if it == 7 else 9,
+                                  kind=("normal", "mixed", "steps", "smooth")[it % 4])
+        got, want = run_pair(cgx, port, c, OP_ENO, CELL, order_space, ntl, fma, rng, form)
+        assert bits_equal(got, want)
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("fma", [False, True], ids=["exact", "fma"])
 def test_restrict_and_copy(cgx, port, fma, form):
     rng = np.random.default_rng(4000)
     for it in range(10):
