@@ -313,6 +313,16 @@ int build_spatial(int op, int cent, const cgx_array *dst, const cgx_array *src,
                                 "order_space not in {2,3,4,5}");
       kind = K_PROLONG_CC_ENO;
       order_space = order_space == 5 ? 3 : 2;
+    } else if (op == CGX_OP_WENO) {
+      // data.cc:722-752: vertex-centred order 5 runs the ENO operator
+      if (cent == CGX_CELL)
+        return fail(CGX_EINVAL, "There are currently no cell-centred stencils for op=\"WENO\"");
+      if (cent != CGX_VERTEX) return fail(CGX_EINVAL, "transfer_prolongate: bad centering");
+      if (order_space == 1 || order_space == 3)
+        return fail(CGX_EINVAL, "There is no stencil for op=\"WENO\" with order_space=%d", order_space);
+      if (order_space != 5)
+        return fail(CGX_EINVAL, "There is no stencil for op=\"WENO\" with order_space!=5");
+      kind = K_PROLONG_ENO;
     } else if (op == CGX_OP_ENO) {
       if (cent != CGX_VERTEX) return fail(CGX_EINVAL, "transfer_prolongate: bad centering");
       if (order_space != 3 && order_space != 5) // data.cc:660-686

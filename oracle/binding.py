@@ -29,7 +29,7 @@ REF_PATH = os.path.join(HERE, "_ref", "libcarpetref.so")
 REF_FMA_PATH = os.path.join(HERE, "_ref", "libcarpetref_fma.so")
 
 # operator_type (CarpetLib/src/operators.hh:8-25)
-OP_ERROR, OP_NONE, OP_SYNC, OP_RESTRICT, OP_COPY, OP_LAGRANGE, OP_ENO = range(7)
+OP_ERROR, OP_NONE, OP_SYNC, OP_RESTRICT, OP_COPY, OP_LAGRANGE, OP_ENO, OP_WENO = range(8)
 # centering (CarpetLib/src/defs.hh:134)
 VERTEX, CELL = 1, 2
 

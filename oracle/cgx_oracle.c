@@ -1085,6 +1085,18 @@ static int transfer_p_r(int fma_, int op, int cent, double *dst,
                                       dstext, srcbbox, dstbbox, srcbox, dstbox);
       return fail(CGXO_EINVAL, "transfer_prolongate: no ENO stencil for this order");
     }
+    if (op == op_WENO) {
+      /* data.cc:722-752: vertex-centred order 5 runs the ENO operator */
+      if (cent == cell_centered)
+        return fail(CGXO_EINVAL, "There are currently no cell-centred stencils for op=\"WENO\"");
+      if (cent != vertex_centered) return fail(CGXO_EINVAL, "transfer_prolongate: bad centering");
+      if (order_space == 1 || order_space == 3)
+        return fail(CGXO_EINVAL, "There is no stencil for op=\"WENO\" with order_space=%d", order_space);
+      if (order_space != 5)
+        return fail(CGXO_EINVAL, "There is no stencil for op=\"WENO\" with order_space!=5");
+      return cgxo_prolongate_3d_eno(fma_, src, srcpadext, srcext, dst, dstpadext, dstext,
+                                    srcbbox, dstbbox, srcbox, dstbox);
+    }
     if (op == op_ENO && cent == cell_centered) {
       /* data.cc:689-720: orders 2-4 run the second-order stencil, 5 the third */
       if (order_space < 2 || order_space > 5)

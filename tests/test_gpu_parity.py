@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from oracle import cases
-from oracle.binding import OP_COPY, OP_ENO, OP_LAGRANGE, CELL, VERTEX, OracleError, alloc
+from oracle.binding import OP_COPY, OP_ENO, OP_LAGRANGE, OP_WENO, CELL, VERTEX, OracleError, alloc
 
 pytestmark = pytest.mark.gpu
 
@@ -120,6 +120,17 @@ def test_vc_eno(cgx, port, ntl, fma, form):
         c = cases.vc_prolong_case(rng, 3, reach=(1, 2), max_ext=40 if it == 7 else 9,
                                   kind=("normal", "steps", "mixed")[it % 3])
         got, want = run_pair(cgx, port, c, OP_ENO, VERTEX, 3, ntl, fma, rng, form)
+        assert bits_equal(got, want)
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("ntl", [1, 2, 3])
+def test_vc_weno(cgx, port, ntl, form):
+    """op WENO, vertex-centred order 5: the ENO operator (data.cc:722-752)"""
+    rng = np.random.default_rng(3050 + ntl)
+    for it in range(4):
+        c = cases.vc_prolong_case(rng, 3, reach=(1, 2), max_ext=9, kind=("steps", "mixed")[it % 2])
+        got, want = run_pair(cgx, port, c, OP_WENO, VERTEX, 5, ntl, False, rng, form)
         assert bits_equal(got, want)
 
 

@@ -401,3 +401,23 @@ def test_cc_eno_order_selection(port):
         with pytest.raises(OracleError, match="order_space not in"):
             port.transfer(OP_ENO, CELL, c["dst"].copy(), c["dstbbox"], [c["src"]], c["srcbbox"],
                           [0.0], c["reg"], c["srcbbox"], 0.0, order_space, 0)
+
+
+def test_weno_prolongation_is_eno(port):
+    """transfer_prolongate's WENO entries (data.cc:722-752): vertex-centred
+    order 5 runs the ENO operator, every other order and cell centring is an
+    error"""
+    from oracle.binding import OP_WENO
+    rng = np.random.default_rng(530)
+    c = cases.vc_prolong_case(rng, 3, reach=(1, 2), max_ext=7, kind="steps")
+    want = c["dst"].copy()
+    port.prolongate_3d_eno(c["src"], c["srcbbox"], want, c["dstbbox"], c["reg"])
+    d = c["dst"].copy()
+    port.transfer(OP_WENO, VERTEX, d, c["dstbbox"], [c["src"]], c["srcbbox"], [0.0], c["reg"],
+                  c["srcbbox"], 0.0, 5, 0)
+    assert bits_equal(d, want)
+    for cent, order, msg in ((VERTEX, 1, "order_space=1"), (VERTEX, 3, "order_space=3"),
+                             (VERTEX, 7, "order_space!=5"), (CELL, 5, "no cell-centred")):
+        with pytest.raises(OracleError, match=msg):
+            port.transfer(OP_WENO, cent, c["dst"].copy(), c["dstbbox"], [c["src"]], c["srcbbox"],
+                          [0.0], c["reg"], c["srcbbox"], 0.0, order, 0)
