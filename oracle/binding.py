@@ -141,6 +141,14 @@ class Port:
         self._ti(self.lib.cgxo_interpolate_eno_3d_3tl, srcs, times, srcbbox, dst,
                  dstbbox, reg, t, fma)
 
+    def interpolate_3d_4tl(self, srcs, times, srcbbox, dst, dstbbox, reg, t, fma=False):
+        self._ti(self.lib.cgxo_interpolate_3d_4tl, srcs, times, srcbbox, dst,
+                 dstbbox, reg, t, fma)
+
+    def interpolate_3d_5tl(self, srcs, times, srcbbox, dst, dstbbox, reg, t, fma=False):
+        self._ti(self.lib.cgxo_interpolate_3d_5tl, srcs, times, srcbbox, dst,
+                 dstbbox, reg, t, fma)
+
     def find_source_timelevel(self, times, time, order_time, op):
         tl0, ntl = C.c_int(), C.c_int()
         ts = (C.c_double * len(times))(*times)
@@ -151,7 +159,7 @@ class Port:
 
     def time_weights(self, kind, times, t):
         w = (C.c_double * 8)()
-        ts = (C.c_double * 3)(*list(times) + [0.0] * (3 - len(times)))
+        ts = (C.c_double * 5)(*list(times) + [0.0] * (5 - len(times)))
         self._check(self.lib.cgxo_time_weights(kind, ts, C.c_double(t), w))
         return list(w)
 
@@ -245,6 +253,14 @@ class Ref:
 
     def interpolate_eno_3d_3tl(self, srcs, times, srcbbox, dst, dstbbox, reg, t):
         self._ti(self.lib.cgxref_interpolate_eno_3d_3tl, srcs, times, srcbbox, dst,
+                 dstbbox, reg, t)
+
+    def interpolate_3d_4tl(self, srcs, times, srcbbox, dst, dstbbox, reg, t):
+        self._ti(self.lib.cgxref_interpolate_3d_4tl, srcs, times, srcbbox, dst,
+                 dstbbox, reg, t)
+
+    def interpolate_3d_5tl(self, srcs, times, srcbbox, dst, dstbbox, reg, t):
+        self._ti(self.lib.cgxref_interpolate_3d_5tl, srcs, times, srcbbox, dst,
                  dstbbox, reg, t)
 
 

@@ -879,6 +879,30 @@ static int ti_region(const box_t *srcbbox, const box_t *dstbbox, const box_t *re
  * (w[0..2] the 3-point weights, w[3..4] the (1,2) pair, w[5..6] the (2,3)
  * pair, w[7] = use_12). */
 int cgxo_time_weights(int kind, const double *ts, double t, double *w) {
+  if (kind == 4 || kind == 5) {
+    /* interpolate_3d_4tl.cc:95-117, interpolate_3d_5tl.cc:100-123: Lagrange
+     * in time, numerator and denominator products left to right */
+    const int n = kind;
+    const double eps = 1.0e-12;
+    const char *who = n == 4 ? "interpolate_3d_4tl" : "interpolate_3d_5tl";
+    for (int i = 0; i < n; ++i)
+      for (int j = i + 1; j < n; ++j)
+        if (fabs(ts[i] - ts[j]) < eps) return fail(CGXO_EINVAL, "%s: arrays have same time", who);
+    double mn = ts[0], mx = ts[0];
+    for (int i = 1; i < n; ++i) { mn = fmin(mn, ts[i]); mx = fmax(mx, ts[i]); }
+    if (t < mn - eps || t > mx + eps) return fail(CGXO_EINVAL, "%s: extrapolation in time", who);
+    for (int i = 0; i < n; ++i) {
+      double num = 0, den = 0;
+      int first = 1;
+      for (int j = 0; j < n; ++j) {
+        if (j == i) continue;
+        if (first) { num = t - ts[j]; den = ts[i] - ts[j]; first = 0; }
+        else { num = num * (t - ts[j]); den = den * (ts[i] - ts[j]); }
+      }
+      w[i] = num / den;
+    }
+    return CGXO_OK;
+  }
   if (kind == 1) {
     double t1 = ts[0], t2 = ts[1], eps = 1.0e-12;
     if (fabs(t1 - t2) < eps) return fail(CGXO_EINVAL, "interpolate_3d_2tl: arrays have same time");
@@ -943,6 +967,8 @@ static int time_interp(int kind, int fma_, const double *const *srcs,
   int regext[3], srcoff[3], dstoff[3], rc;
   const char *who = kind == 1 ? "interpolate_3d_2tl" : kind == 2 ? "interpolate_3d_3tl"
                                                                  : "interpolate_eno_3d_3tl";
+  if (kind == 4) who = "interpolate_3d_4tl";
+  if (kind == 5) who = "interpolate_3d_5tl";
   if ((rc = ti_region(&srcbbox, &dstbbox, &reg, regext, srcoff, dstoff, who))) return rc;
   double w[8];
   if ((rc = cgxo_time_weights(kind, ts, t, w))) return rc;
@@ -953,7 +979,12 @@ static int time_interp(int kind, int fma_, const double *const *srcs,
         double r;
         if (kind == 1) r = tcomb2(fma_, w[0], srcs[0][si], w[1], srcs[1][si]);
         else if (kind == 2) r = tcomb3(fma_, w[0], srcs[0][si], w[1], srcs[1][si], w[2], srcs[2][si]);
-        else r = teno(fma_, w, srcs[0][si], srcs[1][si], srcs[2][si]);
+        else if (kind == 3) r = teno(fma_, w, srcs[0][si], srcs[1][si], srcs[2][si]);
+        else {
+          /* s1*a + s2*b + s3*c + s4*d (+ s5*e), left to right */
+          r = tcomb3(fma_, w[0], srcs[0][si], w[1], srcs[1][si], w[2], srcs[2][si]);
+          for (int m = 3; m < kind; ++m) r = madd(fma_, w[m], srcs[m][si], r);
+        }
         dst[IDX(dstoff[0] + i, dstoff[1] + j, dstoff[2] + k, dstpadext)] = r;
       }
   return CGXO_OK;
@@ -983,6 +1014,33 @@ int cgxo_interpolate_3d_3tl(int fma_, const double *src1, double t1,
   const double *s[3] = {src1, src2, src3};
   double ts[3] = {t1, t2, t3};
   return time_interp(2, fma_, s, ts, srcpadext, dst, t, dstpadext, srcbbox, dstbbox, regbbox);
+}
+/* interpolate_3d_4tl, CarpetLib/src/interpolate_3d_4tl.cc:24-134 */
+int cgxo_interpolate_3d_4tl(int fma_, const double *src1, double t1,
+                            const double *src2, double t2, const double *src3,
+                            double t3, const double *src4, double t4,
+                            const int *srcpadext, const int *srcext, double *dst,
+                            double t, const int *dstpadext, const int *dstext,
+                            const int *srcbbox, const int *dstbbox,
+                            const int *srcregbbox, const int *regbbox) {
+  (void)srcext; (void)dstext; (void)srcregbbox;
+  const double *s[4] = {src1, src2, src3, src4};
+  double ts[4] = {t1, t2, t3, t4};
+  return time_interp(4, fma_, s, ts, srcpadext, dst, t, dstpadext, srcbbox, dstbbox, regbbox);
+}
+/* interpolate_3d_5tl, CarpetLib/src/interpolate_3d_5tl.cc:24-139 */
+int cgxo_interpolate_3d_5tl(int fma_, const double *src1, double t1,
+                            const double *src2, double t2, const double *src3,
+                            double t3, const double *src4, double t4,
+                            const double *src5, double t5, const int *srcpadext,
+                            const int *srcext, double *dst, double t,
+                            const int *dstpadext, const int *dstext,
+                            const int *srcbbox, const int *dstbbox,
+                            const int *srcregbbox, const int *regbbox) {
+  (void)srcext; (void)dstext; (void)srcregbbox;
+  const double *s[5] = {src1, src2, src3, src4, src5};
+  double ts[5] = {t1, t2, t3, t4, t5};
+  return time_interp(5, fma_, s, ts, srcpadext, dst, t, dstpadext, srcbbox, dstbbox, regbbox);
 }
 /* interpolate_eno_3d_3tl, CarpetLib/src/interpolate_eno_3d_3tl.cc:32-165 */
 int cgxo_interpolate_eno_3d_3tl(int fma_, const double *src1, double t1,
@@ -1163,7 +1221,10 @@ int cgxo_transfer(int fma_, int op, int cent, double *dst, const int *dstpadext,
   sizes_of(dstbox, ext);
   size_t npts = (size_t)ext[0] * ext[1] * ext[2];
   double *tmp[5] = {0};
-  if (ntl > 3) return fail(CGXO_EUNSUPPORTED, "time_interpolate: order_time > 2");
+  if (ntl > 5) return fail(CGXO_EINVAL, "time_interpolate: order_time > 4");
+  if (ntl > 3 && !(op == op_copy || op == op_Lagrange)) /* data.cc:1295-1297 */
+    return fail(CGXO_EINVAL, "time_interpolate: no ENO-family interpolation of order_time %d",
+                order_time);
   for (int tl = 0; tl < ntl; ++tl) {
     tmp[tl] = (double *)malloc(npts * sizeof(double) + 8);
     if (!tmp[tl]) { rc = fail(CGXO_ENOMEM, "out of memory"); goto done; }
@@ -1182,10 +1243,18 @@ int cgxo_transfer(int fma_, int op, int cent, double *dst, const int *dstpadext,
     if (order_time == 1)
       rc = cgxo_interpolate_3d_2tl(fma_, tmp[0], ts[0], tmp[1], ts[1], ext, ext, dst, time,
                                    dstpadext, dext, dstbox, dstbbox, dstbox, dstbox);
-    else if (lagr)
+    else if (lagr && order_time == 2)
       rc = cgxo_interpolate_3d_3tl(fma_, tmp[0], ts[0], tmp[1], ts[1], tmp[2], ts[2], ext,
                                    ext, dst, time, dstpadext, dext, dstbox, dstbbox, dstbox,
                                    dstbox);
+    else if (lagr && order_time == 3)
+      rc = cgxo_interpolate_3d_4tl(fma_, tmp[0], ts[0], tmp[1], ts[1], tmp[2], ts[2], tmp[3],
+                                   ts[3], ext, ext, dst, time, dstpadext, dext, dstbox,
+                                   dstbbox, dstbox, dstbox);
+    else if (lagr)
+      rc = cgxo_interpolate_3d_5tl(fma_, tmp[0], ts[0], tmp[1], ts[1], tmp[2], ts[2], tmp[3],
+                                   ts[3], tmp[4], ts[4], ext, ext, dst, time, dstpadext, dext,
+                                   dstbox, dstbbox, dstbox, dstbox);
     else
       rc = cgxo_interpolate_eno_3d_3tl(fma_, tmp[0], ts[0], tmp[1], ts[1], tmp[2], ts[2],
                                        ext, ext, dst, time, dstpadext, dext, dstbox,

@@ -208,6 +208,24 @@ int cgxref_interpolate_3d_3tl(const double *src1, double t1,
   });
 }
 
+// interpolate_3d_4tl (CarpetLib/src/interpolate_3d_4tl.cc:24)
+int cgxref_interpolate_3d_4tl(const double *src1, double t1, const double *src2, double t2,
+                              const double *src3, double t3, const double *src4, double t4,
+                              TIARGS) {
+  return guarded([&] {
+    interpolate_3d_4tl<double>(src1, t1, src2, t2, src3, t3, src4, t4, TICALL);
+  });
+}
+
+// interpolate_3d_5tl (CarpetLib/src/interpolate_3d_5tl.cc:24)
+int cgxref_interpolate_3d_5tl(const double *src1, double t1, const double *src2, double t2,
+                              const double *src3, double t3, const double *src4, double t4,
+                              const double *src5, double t5, TIARGS) {
+  return guarded([&] {
+    interpolate_3d_5tl<double>(src1, t1, src2, t2, src3, t3, src4, t4, src5, t5, TICALL);
+  });
+}
+
 // interpolate_eno_3d_3tl (CarpetLib/src/interpolate_eno_3d_3tl.cc:32)
 int cgxref_interpolate_eno_3d_3tl(const double *src1, double t1,
                                   const double *src2, double t2,

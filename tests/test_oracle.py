@@ -421,3 +421,66 @@ def test_weno_prolongation_is_eno(port):
         with pytest.raises(OracleError, match=msg):
             port.transfer(OP_WENO, cent, c["dst"].copy(), c["dstbbox"], [c["src"]], c["srcbbox"],
                           [0.0], c["reg"], c["srcbbox"], 0.0, order, 0)
+
+
+# ---------------------------------------------------------------- 4 and 5 timelevels
+@needs_ref
+@pytest.mark.parametrize("ntl", [4, 5])
+def test_interpolate_4tl_5tl_bit_exact_vs_reference(port, ntl):
+    """interpolate_3d_4tl / interpolate_3d_5tl (order_time 3 and 4)"""
+    ref = Ref(False)
+    rng = np.random.default_rng(700 + ntl)
+    fn = f"interpolate_3d_{ntl}tl"
+    for it in range(20):
+        c = cases.time_case(rng, ntl, kind=("normal", "mixed")[it % 2])
+        d1, d2 = c["dst"].copy(), c["dst"].copy()
+        getattr(port, fn)(c["srcs"], c["times"], c["srcbbox"], d1, c["dstbbox"], c["reg"], c["t"])
+        getattr(ref, fn)(c["srcs"], c["times"], c["srcbbox"], d2, c["dstbbox"], c["reg"], c["t"])
+        assert bits_equal(d1, d2)
+    c = cases.time_case(rng, ntl)
+    for lib in (port, ref):
+        with pytest.raises(OracleError):  # extrapolation in time
+            getattr(lib, fn)(c["srcs"], c["times"], c["srcbbox"], c["dst"].copy(), c["dstbbox"],
+                             c["reg"], c["times"][0] + 1.0)
+        with pytest.raises(OracleError):  # coincident times
+            getattr(lib, fn)(c["srcs"], [0.0, -1.0, -1.0, -2.0, -3.0][:ntl], c["srcbbox"],
+                             c["dst"].copy(), c["dstbbox"], c["reg"], -0.5)
+
+
+@pytest.mark.parametrize("order_time", [3, 4])
+def test_transfer_high_order_time_and_restriction_in_time(port, order_time):
+    """transfer_time with order_time 3 / 4, and restriction between
+    timelevels: the spatial operator per timelevel into temporaries, then
+    interpolate_3d_{4,5}tl (or 2tl / 3tl for the restriction)"""
+    rng = np.random.default_rng(710 + order_time)
+    ntl = order_time + 1
+    times = [1.0 - 0.25 * i for i in range(ntl)]
+    t = 0.8
+    c = cases.vc_prolong_case(rng, 5, max_ext=6, kind="mixed")
+    srcs = [c["src"] * (1.0 + 0.5 * i) - i for i in range(ntl)]
+    d = c["dst"].copy()
+    port.transfer(OP_LAGRANGE, VERTEX, d, c["dstbbox"], srcs, c["srcbbox"], times, c["reg"],
+                  c["srcbbox"], t, 5, order_time)
+    reg = c["reg"]
+    tmps = [alloc(reg, pad_x_even=False) for _ in srcs]
+    for s, tm in zip(srcs, tmps):
+        port.prolongate_3d_rf2(5, s, c["srcbbox"], tm, reg, reg)
+    d2 = c["dst"].copy()
+    getattr(port, f"interpolate_3d_{ntl}tl")(tmps, times, reg, d2, c["dstbbox"], reg, t)
+    assert bits_equal(d, d2)
+    # the ENO family has no interpolation beyond order_time 2 (data.cc:1295-1297)
+    with pytest.raises(OracleError, match="order_time"):
+        port.transfer(OP_ENO, VERTEX, c["dst"].copy(), c["dstbbox"], srcs, c["srcbbox"], times,
+                      c["reg"], c["srcbbox"], t, 3, order_time)
+    # restriction at a time between timelevels (order_time 2: three timelevels)
+    r = cases.cc_restrict_case(rng, kind="mixed")
+    rs = [r["src"] * (1.0 + i) for i in range(3)]
+    d = r["dst"].copy()
+    port.transfer(OP_LAGRANGE, CELL, d, r["dstbbox"], rs, r["srcbbox"], times[:3], r["reg"],
+                  r["srcbbox"], t, 1, 2)
+    tmps = [alloc(r["reg"], pad_x_even=False) for _ in rs]
+    for s, tm in zip(rs, tmps):
+        port.restrict_3d_cc_rf2(s, r["srcbbox"], tm, r["reg"], r["reg"])
+    d2 = r["dst"].copy()
+    port.interpolate_3d_3tl(tmps, times[:3], r["reg"], d2, r["dstbbox"], r["reg"], t)
+    assert bits_equal(d, d2)
