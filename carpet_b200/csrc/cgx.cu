@@ -172,6 +172,31 @@ int find_tl(const double *times, int ntimes, double time, int order_time, int op
   return CGX_OK;
 }
 
+// interpolate_3d_4tl.cc:95-117, interpolate_3d_5tl.cc:100-123: Lagrange
+// weights of n = 4 or 5 timelevels, numerator and denominator products
+// formed left to right.
+int lag_weights(int n, const double *ts, double t, double *w) {
+  const double eps = 1.0e-12;
+  const char *who = n == 4 ? "interpolate_3d_4tl" : "interpolate_3d_5tl";
+  for (int i = 0; i < n; ++i)
+    for (int j = i + 1; j < n; ++j)
+      if (std::fabs(ts[i] - ts[j]) < eps) return fail(CGX_EINVAL, "%s: arrays have same time", who);
+  double mn = ts[0], mx = ts[0];
+  for (int i = 1; i < n; ++i) { mn = std::fmin(mn, ts[i]); mx = std::fmax(mx, ts[i]); }
+  if (t < mn - eps || t > mx + eps) return fail(CGX_EINVAL, "%s: extrapolation in time", who);
+  for (int i = 0; i < n; ++i) {
+    double num = 0.0, den = 0.0;
+    bool first = true;
+    for (int j = 0; j < n; ++j) {
+      if (j == i) continue;
+      if (first) { num = t - ts[j]; den = ts[i] - ts[j]; first = false; }
+      else { num = num * (t - ts[j]); den = den * (ts[i] - ts[j]); }
+    }
+    w[i] = num / den;
+  }
+  return CGX_OK;
+}
+
 // Time weights exactly as the reference computes them (once per call):
 // interpolate_3d_2tl.cc:232-242, interpolate_3d_3tl.cc:365-382,
 // interpolate_eno_3d_3tl.cc:105-135.
@@ -230,12 +255,26 @@ void stencil_range(const Win &w, int soff, int n, int *cmin, int *cmax) {
   *cmax = mx;
 }
 
+// One box-pair.  With nst > 0 the pair runs transfer_time in its two
+// stages (data.cc:506-517): st[t] writes timelevel t's spatial result into
+// a temporary of the region's shape, and d (K_TIME) combines the nst
+// temporaries into the destination.  The temporaries are bound by bind_tmp.
 struct Built {
   Desc d;
   long long bytes;  // algorithmic bytes (reads + writes)
   long long points; // destination points written
   int ntiles;
+  int nst;            // timelevels staged through temporaries, or 0
+  Desc st[5];
+  int st_ntiles;
+  long long tmp_elems; // doubles of temporaries
 };
+
+void bind_tmp(Built &b, double *tmp) {
+  const long long npts = b.tmp_elems / b.nst;
+  for (int t = 0; t < b.nst; ++t) b.st[t].dst = tmp + t * npts;
+  for (int t = 0; t < 3; ++t) b.d.src[t] = tmp;
+}
 
 bool pad_ok(const cgx_array *a) {
   Box b(a->bbox);
@@ -534,8 +573,14 @@ int build(int op, int cent, const cgx_array *dst, const cgx_array *srcs, const d
     if (!lagr && !eno) return fail(CGX_EINVAL, "time_interpolate: bad operator");
     if (order_time == 1) tk = T_LIN;
     else if (order_time == 2) tk = lagr ? T_QUAD : T_ENO;
-    else return fail(CGX_EUNSUPPORTED, "time_interpolate: order_time %d is not provided", order_time);
-    if ((rc = time_weights(tk, times + tl0, time, d.w))) return rc;
+    else if (order_time <= 4) {
+      if (!lagr) // data.cc:1295-1297
+        return fail(CGX_EINVAL, "time_interpolate: no ENO-family interpolation of order_time %d",
+                    order_time);
+      tk = T_LAG;
+    } else return fail(CGX_EINVAL, "time_interpolate: order_time %d", order_time);
+    rc = tk == T_LAG ? lag_weights(ntl, times + tl0, time, d.w) : time_weights(tk, times + tl0, time, d.w);
+    if (rc) return rc;
   }
   d.ntl = ntl;
   d.tkind = tk;
@@ -548,10 +593,52 @@ int build(int op, int cent, const cgx_array *dst, const cgx_array *srcs, const d
   // read once (copy and restrictions counted per point above)
   const long long src_bytes = b.bytes - 8 * b.points; // one timelevel's reads
   b.bytes = 8 * b.points + (long long)ntl * src_bytes;
+  // the fused kernels interpolate up to 3 timelevels after copies and
+  // prolongations; restrictions between timelevels and 4 or 5 timelevels
+  // run the reference's two stages
+  if (ntl > 3 || (ntl > 1 && !(d.kind == K_COPY || is_stencil(d.kind)))) {
+    const long long npts = (long long)d.n[0] * d.n[1] * d.n[2];
+    for (int t = 0; t < ntl; ++t) {
+      Desc &s = b.st[t];
+      s = d;
+      s.ntl = 1;
+      s.tkind = T_NONE;
+      for (int q = 0; q < 3; ++q) s.src[q] = srcs[tl0 + t].data;
+      s.dst = nullptr;
+      s.dsy = d.n[0];
+      s.dsz = (long long)d.n[0] * d.n[1];
+      for (int k = 0; k < 3; ++k) s.doff[k] = 0;
+      b.st_ntiles = kind_tiles(s);
+      if (b.st_ntiles <= 0) return fail(CGX_EINVAL, "transfer: region too large");
+    }
+    d.kind = K_TIME;
+    d.order = 0;
+    for (int k = 0; k < 3; ++k) d.soff[k] = 0;
+    for (int q = 0; q < 3; ++q) d.src[q] = nullptr;
+    b.nst = ntl;
+    b.tmp_elems = ntl * npts;
+  }
   b.ntiles = kind_tiles(d);
   if (b.ntiles <= 0) return fail(CGX_EINVAL, "transfer: region too large");
   *out = b;
   return CGX_OK;
+}
+
+int launch_pair(const Desc &d, int ntiles, int fp, int *status, cudaStream_t s);
+
+// The two stages of a staged pair on one stream, with stream-ordered
+// temporaries.
+int launch_staged(Built &b, int fp, int *status, cudaStream_t s) {
+  double *tmp = nullptr;
+  cudaError_t e = cudaMallocAsync(&tmp, (size_t)b.tmp_elems * sizeof(double), s);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
+  bind_tmp(b, tmp);
+  int rc = CGX_OK;
+  for (int t = 0; t < b.nst && rc == CGX_OK; ++t) rc = launch_pair(b.st[t], b.st_ntiles, fp, status, s);
+  if (rc == CGX_OK) rc = launch_pair(b.d, b.ntiles, fp, status, s);
+  e = cudaFreeAsync(tmp, s);
+  if (rc == CGX_OK && e != cudaSuccess) rc = cuda_fail(e, "cudaFreeAsync");
+  return rc;
 }
 
 int launch_pair(const Desc &d, int ntiles, int fp, int *status, cudaStream_t s) {
@@ -639,7 +726,57 @@ struct cgx_batch {
   unsigned long long *d_counter = nullptr; // one per tile-map segment
   int *d_status = nullptr;
   int fp_mode = CGX_FP_EXACT;
+  // staged pairs: offsets (doubles) into the batch's temporaries of a
+  // descriptor's destination (stage 1) or sources (stage 2), else -1
+  std::vector<long long> tdst, tsrc;
+  long long tmp_elems = 0;
+  int nstage1 = 0;       // stage-1 descriptors (not pairs of their own)
+  double *d_tmp = nullptr;
+  size_t tmp_cap = 0;    // doubles
+  std::vector<Desc> pdescs; // descs with the temporaries bound
 };
+
+namespace {
+void batch_push(cgx_batch *b, const Desc &d, long long bytes, long long points, int ntiles,
+                long long tdst, long long tsrc) {
+  b->descs.push_back(d);
+  b->bytes.push_back(bytes);
+  b->points.push_back(points);
+  b->ntiles.push_back(ntiles);
+  b->high.push_back(d.kind == K_PROLONG_VC && d.order >= 7);
+  b->tdst.push_back(tdst);
+  b->tsrc.push_back(tsrc);
+}
+void batch_add_built(cgx_batch *b, const Built &x) {
+  if (!x.nst) {
+    batch_push(b, x.d, x.bytes, x.points, x.ntiles, -1, -1);
+    return;
+  }
+  const long long base = b->tmp_elems, npts = x.tmp_elems / x.nst;
+  for (int t = 0; t < x.nst; ++t) batch_push(b, x.st[t], 0, 0, x.st_ntiles, base + t * npts, -1);
+  batch_push(b, x.d, x.bytes, x.points, x.ntiles, -1, base);
+  b->nstage1 += x.nst;
+  b->tmp_elems += x.tmp_elems;
+}
+// the batch's temporaries, and pdescs: the descriptors with them bound
+int batch_bind(cgx_batch *b) {
+  if ((size_t)b->tmp_elems > b->tmp_cap) {
+    cudaFree(b->d_tmp);
+    b->d_tmp = nullptr;
+    b->tmp_cap = 0;
+    cudaError_t e = cudaMalloc(&b->d_tmp, (size_t)b->tmp_elems * sizeof(double));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc (temporaries)");
+    b->tmp_cap = (size_t)b->tmp_elems;
+  }
+  b->pdescs = b->descs;
+  for (size_t i = 0; i < b->pdescs.size(); ++i) {
+    if (b->tdst[i] >= 0) b->pdescs[i].dst = b->d_tmp + b->tdst[i];
+    if (b->tsrc[i] >= 0)
+      for (int t = 0; t < 3; ++t) b->pdescs[i].src[t] = b->d_tmp + b->tsrc[i];
+  }
+  return CGX_OK;
+}
+} // namespace
 
 struct cgx_graph {
   cudaGraph_t graph = nullptr;
@@ -683,6 +820,7 @@ int cgx_transfer(int op, int cent, const cgx_array *dst, const cgx_array *srcs, 
   int rc = build(op, cent, dst, srcs, times, nsrc, dstbox, srcbox, slab_offset, time, order_space,
                  order_time, &b);
   if (rc) return rc;
+  if (b.nst) return launch_staged(b, g_fp_mode, nullptr, (cudaStream_t)stream);
   return launch_pair(b.d, b.ntiles, g_fp_mode, nullptr, (cudaStream_t)stream);
 }
 
@@ -717,6 +855,7 @@ int cgx_batch_destroy(cgx_batch *b) {
   cudaFree(b->d_maps);
   cudaFree(b->d_counter);
   cudaFree(b->d_status);
+  cudaFree(b->d_tmp);
   delete b;
   return CGX_OK;
 }
@@ -728,6 +867,10 @@ int cgx_batch_clear(cgx_batch *b) {
   b->points.clear();
   b->ntiles.clear();
   b->high.clear();
+  b->tdst.clear();
+  b->tsrc.clear();
+  b->tmp_elems = 0;
+  b->nstage1 = 0;
   return CGX_OK;
 }
 
@@ -739,11 +882,7 @@ int cgx_batch_add(cgx_batch *b, int op, int cent, const cgx_array *dst, const cg
   int rc = build(op, cent, dst, srcs, times, nsrc, dstbox, srcbox, slab_offset, time, order_space,
                  order_time, &x);
   if (rc) return rc;
-  b->descs.push_back(x.d);
-  b->bytes.push_back(x.bytes);
-  b->points.push_back(x.points);
-  b->ntiles.push_back(x.ntiles);
-  b->high.push_back(x.d.kind == K_PROLONG_VC && x.d.order >= 7);
+  batch_add_built(b, x);
   return CGX_OK;
 }
 
@@ -751,22 +890,18 @@ int cgx_batch_add_many(cgx_batch *b, int op, int cent, const cgx_array *arrays, 
                        const int *dst_idx, const int *src_idx, int nsrc, const double *times,
                        const int *dstboxes, const int *srcboxes, double time, int order_space,
                        int order_time) {
-  if (!b || npairs < 0 || nsrc < 1 || nsrc > 3 ||
+  if (!b || npairs < 0 || nsrc < 1 || nsrc > 5 ||
       (npairs > 0 && (!arrays || !dst_idx || !src_idx || !dstboxes || !srcboxes)))
     return fail(CGX_EINVAL, "add_many: bad arguments");
   b->descs.reserve(b->descs.size() + npairs);
-  cgx_array srcs[3];
+  cgx_array srcs[5];
   for (int i = 0; i < npairs; ++i) {
     for (int t = 0; t < nsrc; ++t) srcs[t] = arrays[src_idx[nsrc * i + t]];
     Built x;
     int rc = build(op, cent, &arrays[dst_idx[i]], srcs, times, nsrc, dstboxes + 9 * (size_t)i,
                    srcboxes + 9 * (size_t)i, nullptr, time, order_space, order_time, &x);
     if (rc) return rc;
-    b->descs.push_back(x.d);
-    b->bytes.push_back(x.bytes);
-    b->points.push_back(x.points);
-    b->ntiles.push_back(x.ntiles);
-    b->high.push_back(x.d.kind == K_PROLONG_VC && x.d.order >= 7);
+    batch_add_built(b, x);
   }
   return CGX_OK;
 }
@@ -776,7 +911,7 @@ int cgx_batch_stats(const cgx_batch *b, int64_t *npairs, int64_t *ntiles, int64_
   if (!b) return fail(CGX_EINVAL, "null batch");
   int64_t t = 0, p = 0, by = 0;
   for (size_t i = 0; i < b->descs.size(); ++i) { t += b->ntiles[i]; p += b->points[i]; by += b->bytes[i]; }
-  if (npairs) *npairs = (int64_t)b->descs.size();
+  if (npairs) *npairs = (int64_t)b->descs.size() - b->nstage1;
   if (ntiles) *ntiles = t;
   if (dst_points) *dst_points = p;
   if (bytes) *bytes = by;
@@ -786,6 +921,8 @@ int cgx_batch_stats(const cgx_batch *b, int64_t *npairs, int64_t *ntiles, int64_
 int cgx_batch_upload(cgx_batch *b, void *stream) {
   if (!b) return fail(CGX_EINVAL, "null batch");
   cudaStream_t s = (cudaStream_t)stream;
+  int brc = batch_bind(b);
+  if (brc) return brc;
   // queue order: by tile-map segment (prolongation, then each streaming
   // variant); within a segment, largest work per tile first, so that a
   // persistent kernel's last claims are small ones
@@ -798,7 +935,7 @@ int cgx_batch_upload(cgx_batch *b, void *stream) {
   // prolongation descriptors whose arrays TMA can stage are tiled in their
   // variant's configuration and get tensor maps
   std::vector<CUtensorMap> em(3 * b->descs.size());
-  std::vector<Desc> dq(b->descs);
+  std::vector<Desc> dq(b->pdescs);
   std::vector<long long> ntq(b->ntiles.begin(), b->ntiles.end());
   for (int i : order) {
     if (!is_stencil(dq[i].kind)) continue;
@@ -882,15 +1019,17 @@ int cgx_batch_upload(cgx_batch *b, void *stream) {
 int cgx_batch_launch(cgx_batch *b, void *stream) {
   if (!b) return fail(CGX_EINVAL, "null batch");
   cudaStream_t s = (cudaStream_t)stream;
+  // the per-box descriptors first: a staged pair's first stage may be one,
+  // and its second stage runs in the last segment of the tile map
+  for (int i : b->high_idx) {
+    int rc = launch_pair(b->pdescs[i], b->ntiles[i], b->fp_mode, b->d_status, s);
+    if (rc) return rc;
+  }
   if (b->n_uploaded > 0) {
     cudaError_t e = cudaMemsetAsync(b->d_counter, 0, NSEG * sizeof(unsigned long long), s);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
     int rc = launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, b->seg, b->tma_cfg, b->d_counter,
                         b->d_status, s);
-    if (rc) return rc;
-  }
-  for (int i : b->high_idx) {
-    int rc = launch_pair(b->descs[i], b->ntiles[i], b->fp_mode, b->d_status, s);
     if (rc) return rc;
   }
   return CGX_OK;
@@ -981,8 +1120,11 @@ int cgx_batch_kernels(const cgx_batch *b, int *nkernels) {
 
 int cgx_batch_launch_per_box(cgx_batch *b, void *stream) {
   if (!b) return fail(CGX_EINVAL, "null batch");
-  for (size_t i = 0; i < b->descs.size(); ++i) {
-    int rc = launch_pair(b->descs[i], b->ntiles[i], g_fp_mode, b->d_status, (cudaStream_t)stream);
+  int brc = batch_bind(b);
+  if (brc) return brc;
+  // in queue order: a staged pair's stages follow one another
+  for (size_t i = 0; i < b->pdescs.size(); ++i) {
+    int rc = launch_pair(b->pdescs[i], b->ntiles[i], g_fp_mode, b->d_status, (cudaStream_t)stream);
     if (rc) return rc;
   }
   return CGX_OK;
@@ -1132,6 +1274,10 @@ extern "C" int cgx_transfer_pairs_noalloc(const cgx_pair *pairs, int npairs, voi
       rc = build(p.op, p.cent, &p.dst, p.srcs, p.times, p.nsrc, p.dstbox, p.srcbox,
                  p.has_slab ? p.slab_offset : nullptr, p.time, p.order_space, p.order_time, &b);
       if (rc) return rc;
+      if (b.nst)
+        return fail(CGX_EUNSUPPORTED,
+                    "pair %d: a transfer through per-timelevel temporaries (restriction between "
+                    "timelevels, order_time 3 or 4) is not available without allocation", i0 + i);
       if (b.d.kind == K_PROLONG_VC && b.d.order >= 7)
         return fail(CGX_EUNSUPPORTED,
                     "pair %d: vertex-centred order %d is not available without allocation",
@@ -1163,6 +1309,7 @@ int host_build(int op, int cent, const cgx_array *dst, const cgx_array *srcs, co
   int rc = build(op, cent, dst, srcs, times, nsrc, dstbox, srcbox, slab, time, order_space,
                  order_time, &b);
   if (rc) return rc;
+  if (b.nst) return fail(CGX_EUNSUPPORTED, "a transfer through per-timelevel temporaries");
   out->d = b.d;
   out->bytes = b.bytes;
   out->points = b.points;
@@ -1175,6 +1322,8 @@ int batch_pairs(const cgx_batch *b, const Desc **descs, const int **ntiles, cons
   if (!b) return fail(CGX_EINVAL, "null batch");
   for (size_t i = 0; i < b->high.size(); ++i)
     if (b->high[i]) return fail(CGX_EUNSUPPORTED, "vertex-centred orders 7-11 cannot be served");
+  if (b->nstage1)
+    return fail(CGX_EUNSUPPORTED, "transfers through per-timelevel temporaries cannot be served");
   *descs = b->descs.data();
   *ntiles = b->ntiles.data();
   *points = b->points.data();

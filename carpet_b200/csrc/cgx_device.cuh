@@ -28,10 +28,12 @@ enum Kind : int {
   K_RESTRICT_CC3 = 6, // restrict_3d_cc_o3_rf2 (4x4x4 cells)
   K_RESTRICT_CC5 = 7, // restrict_3d_cc_o5_rf2 (6x6x6 cells, separable)
   K_PROLONG_CC_ENO = 8, // prolongate_3d_cc_eno_rf2<ORDER>, ORDER (d.order) 2 or 3
-  K_NKINDS = 9
+  K_TIME = 9,           // time_interpolate of per-timelevel temporaries
+  K_NKINDS = 10
 };
 
-enum TKind : int { T_NONE = 0, T_LIN = 1, T_QUAD = 2, T_ENO = 3 };
+// T_LAG: interpolate_3d_4tl / interpolate_3d_5tl (ntl 4 or 5)
+enum TKind : int { T_NONE = 0, T_LIN = 1, T_QUAD = 2, T_ENO = 3, T_LAG = 4 };
 
 // Tile geometry.
 constexpr int NTHREADS = 256;
@@ -326,7 +328,8 @@ enum StreamVariant : int {
   SV_RESTRICT_CC = 5, // 8-point average
   SV_RESTRICT_CC3 = 6, // third-order cell-centred restriction
   SV_RESTRICT_CC5 = 7, // fifth-order cell-centred restriction
-  SV_COUNT = 8
+  SV_TIME = 8,         // time combination of temporaries (K_TIME)
+  SV_COUNT = 9
 };
 
 template <class D> __host__ __device__ __forceinline__ int stream_variant(const D &d) {
@@ -334,6 +337,7 @@ template <class D> __host__ __device__ __forceinline__ int stream_variant(const 
   if (d.kind == K_RESTRICT_CC) return SV_RESTRICT_CC;
   if (d.kind == K_RESTRICT_CC3) return SV_RESTRICT_CC3;
   if (d.kind == K_RESTRICT_CC5) return SV_RESTRICT_CC5;
+  if (d.kind == K_TIME) return SV_TIME;
   if (d.kind != K_COPY) return -1;
   if (d.ntl == 1) return SV_COPY1;
   if (d.ntl == 2) return SV_COPY2;
@@ -460,6 +464,44 @@ __device__ __forceinline__ void restrict_cc_tile(const D &d, int tile, int lid) 
     res = madd<FMA>(w, a5, res);
     res = madd<FMA>(w, a6, res);
     res = madd<FMA>(w, a7, res);
+    dst[i + j * d.dsy + k * d.dsz] = res;
+  }
+}
+
+// The second stage of transfer_time (data.cc:506-517) where the fused
+// kernels do not apply: d.src[0] holds d.ntl temporaries of the region's
+// shape, one after another, x fastest and unpadded; time_interpolate
+// (data.cc:1183-1299) combines them into the destination.  4 and 5
+// timelevels sum s1*a + s2*b + s3*c + s4*d (+ s5*e) left to right
+// (interpolate_3d_4tl.cc:126-131, interpolate_3d_5tl.cc:128-132).
+template <int FMA, int LANES, class D>
+__device__ __forceinline__ void time_tile(const D &d, int tile, int lid) {
+  constexpr int PER = STILE / LANES;
+  const unsigned npts = (unsigned)d.n[0] * d.n[1] * d.n[2];
+  const unsigned p0 = (unsigned)tile * STILE + lid;
+  const double *tmp = d.src[0];
+  double *dst = d.dst + (d.doff[0] + d.doff[1] * d.dsy + d.doff[2] * d.dsz);
+  const int ntl = d.ntl, tk = d.tkind;
+  double w[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) w[k] = d.w[k];
+#pragma unroll 2
+  for (int r = 0; r < PER; ++r) {
+    const unsigned p = p0 + r * LANES;
+    if (p >= npts) break;
+    double v[5];
+#pragma unroll
+    for (int t = 0; t < 5; ++t) v[t] = t < ntl ? __ldg(tmp + (size_t)t * npts + p) : 0.0;
+    double res;
+    if (ntl == 2) res = tcombine<FMA, T_LIN, 2>(w, v);
+    else if (ntl == 3 && tk == T_ENO) res = tcombine<FMA, T_ENO, 3>(w, v);
+    else {
+      res = tcombine<FMA, T_QUAD, 3>(w, v);
+      if (ntl >= 4) res = madd<FMA>(w[3], v[3], res);
+      if (ntl == 5) res = madd<FMA>(w[4], v[4], res);
+    }
+    int i, j, k;
+    unflatten(d, p, i, j, k);
     dst[i + j * d.dsy + k * d.dsz] = res;
   }
 }

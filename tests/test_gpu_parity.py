@@ -319,3 +319,116 @@ def test_exact_mode_matches_compiled_reference(cgx):
             cgx.transfer_data(dst, [src], [0.0], c["reg"], c["srcbbox"], 0.0, order, 0)
             torch.cuda.synchronize()
             assert bits_equal(dst.tensor.cpu().numpy(), want)
+
+
+# ---------------------------------------------------------------- two stages
+def timeset5(rng, ntl):
+    """five timelevels t0, t0-dt, ...; a time that selects the first ntl
+    (order_time = ntl - 1)"""
+    t0, dt = float(rng.uniform(-1, 1)), float(rng.uniform(0.05, 0.5))
+    times = [t0 - i * dt for i in range(5)]
+    if ntl == 1:  # an exact match selects one timelevel
+        return times, times[int(rng.integers(0, 5))], 2
+    return times, float(rng.uniform(times[ntl - 1] + 1e-3, times[0] - 1e-3)), ntl - 1
+
+
+def staged_cases(rng, big=False):
+    """(case, op, cent, order_space, ntl): transfers that run through
+    per-timelevel temporaries"""
+    m = 30 if big else 8
+    out = []
+    for ntl in (4, 5):
+        out.append((cases.vc_prolong_case(rng, 5, max_ext=m, kind="mixed"), OP_LAGRANGE, VERTEX, 5, ntl))
+        out.append((cases.cc_prolong_case(rng, 3, max_ext=m, kind="mixed"), OP_LAGRANGE, CELL, 3, ntl))
+        out.append((cases.copy_case(rng, max_ext=m, kind="mixed"), OP_LAGRANGE, VERTEX, 1, ntl))
+        out.append((cases.vc_prolong_case(rng, 7, max_ext=m, kind="mixed"), OP_LAGRANGE, VERTEX, 7, ntl))
+    for ntl in (2, 3):
+        out.append((cases.vc_restrict_case(rng, max_ext=m, kind="mixed"), OP_LAGRANGE, VERTEX, 1, ntl))
+        out.append((cases.cc_restrict_case(rng, max_ext=m, kind="mixed"), OP_LAGRANGE, CELL, 1, ntl))
+        out.append((cases.cc_restrict_case(rng, max_ext=m, kind="mixed"), OP_ENO, CELL, 1, ntl))
+    return out
+
+
+def staged_io(cb, port, c, op, cent, order, ntl, fma, rng):
+    times, time, ot = timeset5(rng, ntl)
+    srcs_np = [c["src"] * (1.0 + 0.25 * i) - 0.5 * i for i in range(5)]
+    reg = c.get("reg", c.get("dstreg"))
+    want = c["dst"].copy()
+    port.transfer(op, cent, want, c["dstbbox"], srcs_np, c["srcbbox"], times, reg, c["srcbbox"],
+                  time, order, ot, fma=fma)
+    dst = to_dev(cb, c["dst"], c["dstbbox"])
+    srcs = [to_dev(cb, s, c["srcbbox"]) for s in srcs_np]
+    return dict(dst=dst, srcs=srcs, times=times, time=time, ot=ot, reg=reg, want=want, init=c["dst"])
+
+
+@pytest.mark.parametrize("fma", [False, True], ids=["exact", "fma"])
+def test_staged_transfers_per_box(cgx, port, fma):
+    """order_time 3 and 4 (interpolate_3d_4tl / 5tl) and restriction between
+    timelevels: the spatial operator per timelevel into temporaries, then
+    the time combination, as transfer_time does"""
+    rng = np.random.default_rng(6000 + fma)
+    cgx.set_fp_mode(fma)
+    for big in (False, True):
+        for c, op, cent, order, ntl in staged_cases(rng, big):
+            x = staged_io(cgx, port, c, op, cent, order, ntl, fma, rng)
+            cgx.transfer_data(x["dst"], x["srcs"], x["times"], x["reg"], c["srcbbox"], x["time"],
+                              order, x["ot"], op=op, cent=cent)
+            torch.cuda.synchronize()
+            got = x["dst"].tensor.cpu().numpy()[:, :, :x["want"].shape[2]]
+            assert bits_equal(got, x["want"]), (op, cent, order, ntl)
+
+
+@pytest.mark.parametrize("fma", [False, True], ids=["exact", "fma"])
+def test_staged_transfers_batched(cgx, port, fma):
+    """staged pairs mixed with fused ones in one batch: the batch's
+    persistent kernels, the per-box launches and a CUDA-graph replay"""
+    rng = np.random.default_rng(6100 + fma)
+    cgx.set_fp_mode(fma)
+    b = cgx.Batch()
+    items = []
+    for c, op, cent, order, ntl in staged_cases(rng):
+        x = staged_io(cgx, port, c, op, cent, order, ntl, fma, rng)
+        b.add(x["dst"], x["srcs"], x["times"], x["reg"], c["srcbbox"], x["time"], order, x["ot"],
+              op=op, cent=cent)
+        items.append(x)
+    for it in range(6):  # fused pairs alongside
+        c = cases.vc_prolong_case(rng, 5, max_ext=12, kind="mixed")
+        x = staged_io(cgx, port, c, OP_LAGRANGE, VERTEX, 5, 1 + it % 3, fma, rng)
+        b.add(x["dst"], x["srcs"], x["times"], x["reg"], c["srcbbox"], x["time"], 5, x["ot"],
+              op=OP_LAGRANGE, cent=VERTEX)
+        items.append(x)
+    assert b.stats()["pairs"] == len(items)
+    b.upload()
+    for mode in ("batch", "per_box", "graph"):
+        for x in items:
+            x["dst"].tensor.copy_(torch.from_numpy(x["init"]))
+        if mode == "batch":
+            b.launch()
+        elif mode == "per_box":
+            b.launch_per_box()
+        else:
+            s = torch.cuda.Stream()
+            g = cgx.Graph()
+            torch.cuda.synchronize()
+            with g.capture(s):
+                b.launch(s)
+            g.launch(s)
+            s.synchronize()
+        b.check()
+        torch.cuda.synchronize()
+        for x in items:
+            got = x["dst"].tensor.cpu().numpy()[:, :, :x["want"].shape[2]]
+            assert bits_equal(got, x["want"]), mode
+
+
+def test_staged_eno_family_beyond_order_time_2_is_refused(cgx, port):
+    rng = np.random.default_rng(6200)
+    c = cases.vc_prolong_case(rng, 3, reach=(1, 2), kind="mixed")
+    times, time, ot = timeset5(rng, 4)
+    srcs = [c["src"]] * 5
+    with pytest.raises(OracleError, match="order_time"):
+        port.transfer(OP_ENO, VERTEX, c["dst"].copy(), c["dstbbox"], srcs, c["srcbbox"], times,
+                      c["reg"], c["srcbbox"], time, 3, ot)
+    with pytest.raises(cgx.CgxError, match="order_time"):
+        cgx.transfer_data(to_dev(cgx, c["dst"], c["dstbbox"]), [to_dev(cgx, s, c["srcbbox"]) for s in srcs],
+                          times, c["reg"], c["srcbbox"], time, 3, ot, op=OP_ENO, cent=VERTEX)
