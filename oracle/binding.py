@@ -29,7 +29,8 @@ REF_PATH = os.path.join(HERE, "_ref", "libcarpetref.so")
 REF_FMA_PATH = os.path.join(HERE, "_ref", "libcarpetref_fma.so")
 
 # operator_type (CarpetLib/src/operators.hh:8-25)
-OP_ERROR, OP_NONE, OP_SYNC, OP_RESTRICT, OP_COPY, OP_LAGRANGE, OP_ENO, OP_WENO = range(8)
+OP_ERROR, OP_NONE, OP_SYNC, OP_RESTRICT, OP_COPY, OP_LAGRANGE, OP_ENO, OP_WENO, OP_TVD, \
+    OP_LAGRANGE_MONOTONE = range(10)
 # centering (CarpetLib/src/defs.hh:134)
 VERTEX, CELL = 1, 2
 
@@ -97,6 +98,10 @@ class Port:
     def prolongate_3d_cc_eno_rf2(self, order, src, srcbbox, dst, dstbbox, reg, fma=False):
         self._op(self.lib.cgxo_prolongate_3d_cc_eno_rf2, (order, int(fma)), src,
                  srcbbox, dst, dstbbox, reg, reg)
+
+    def prolongate_3d_o5_monotone_rf2(self, src, srcbbox, dst, dstbbox, reg, fma=False):
+        self._op(self.lib.cgxo_prolongate_3d_o5_monotone_rf2, (int(fma),), src, srcbbox, dst,
+                 dstbbox, reg, reg)
 
     def prolongate_3d_eno(self, src, srcbbox, dst, dstbbox, reg, fma=False):
         self._op(self.lib.cgxo_prolongate_3d_eno, (int(fma),), src, srcbbox, dst,
@@ -215,6 +220,10 @@ class Ref:
 
     def prolongate_3d_cc_rf2(self, order, src, srcbbox, dst, dstbbox, reg):
         self._op(self.lib.cgxref_prolongate_3d_cc_rf2, (order,), src, srcbbox, dst,
+                 dstbbox, reg, reg)
+
+    def prolongate_3d_o5_monotone_rf2(self, src, srcbbox, dst, dstbbox, reg):
+        self._op(self.lib.cgxref_prolongate_3d_o5_monotone_rf2, (), src, srcbbox, dst,
                  dstbbox, reg, reg)
 
     def prolongate_3d_cc_eno_rf2(self, order, src, srcbbox, dst, dstbbox, reg):

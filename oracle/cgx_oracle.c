@@ -655,6 +655,155 @@ int cgxo_prolongate_3d_cc_eno_rf2(int order, int fma_, const double *src,
 }
 
 /* ------------------------------------------------------------------ */
+/* prolongate_3d_o5_monotone_rf2, CarpetLib/src/                        */
+/* prolongate_3d_o5_monotone_rf2.cc:45-793 (op Lagrange_monotone)       */
+
+/* std::min / std::max, argument order kept (NaN and signed-zero ties) */
+static double smin(double a, double b) { return b < a ? b : a; }
+static double smax(double a, double b) { return a < b ? b : a; }
+
+/* The fine point with coarse base b[3] whose odd axes are ax[0..n-1]
+ * (increasing): n = 0 copies; otherwise the tensor-product order-5 stencil
+ * over coarse b-2 .. b+3 on the odd axes, summed left to right with the
+ * lowest odd axis fastest and weight f_a * f_b (* f_c) formed left to
+ * right; with three odd axes each z plane is its own partial sum and the
+ * six are added in order (:499-716).  A result outside the nearest 2/4/8
+ * coarse values (min/max nested as min4/max4/min8/max8, :19-43) falls back
+ * to linear, bilinear or trilinear interpolation. */
+static double mono_point(int fma_, const double *src, const int *pad, const int *b,
+                         const int *ax, int n) {
+  static const double f[6] = {3.0 / 256, -25.0 / 256, 150.0 / 256, 150.0 / 256, -25.0 / 256,
+                              3.0 / 256};
+  const double h = 0.5;
+#define MS(o0, o1, o2) src[IDX(b[0] + (o0), b[1] + (o1), b[2] + (o2), pad)]
+  int e[3][3] = {{0}}; /* unit offset along odd axis m */
+  for (int m = 0; m < n; ++m) e[m][ax[m]] = 1;
+  if (n == 0) return MS(0, 0, 0);
+  double res;
+  if (n == 1) {
+    res = f[0] * MS(-2 * e[0][0], -2 * e[0][1], -2 * e[0][2]);
+    for (int m = 1; m < 6; ++m)
+      res = madd(fma_, f[m], MS((m - 2) * e[0][0], (m - 2) * e[0][1], (m - 2) * e[0][2]), res);
+    double v0 = MS(0, 0, 0), v1 = MS(e[0][0], e[0][1], e[0][2]);
+    if (res > smax(v0, v1) || res < smin(v0, v1)) res = madd(fma_, h, v1, h * v0);
+    return res;
+  }
+  if (n == 2) {
+    res = 0;
+    for (int q = 0; q < 36; ++q) {
+      int m0 = q % 6 - 2, m1 = q / 6 - 2;
+      double w = f[q % 6] * f[q / 6];
+      double v = MS(m0 * e[0][0] + m1 * e[1][0], m0 * e[0][1] + m1 * e[1][1],
+                    m0 * e[0][2] + m1 * e[1][2]);
+      res = q == 0 ? w * v : madd(fma_, w, v, res);
+    }
+    double x1 = MS(0, 0, 0), x2 = MS(e[0][0], e[0][1], e[0][2]), x3 = MS(e[1][0], e[1][1], e[1][2]),
+           x4 = MS(e[0][0] + e[1][0], e[0][1] + e[1][1], e[0][2] + e[1][2]);
+    if (res > smax(smax(x1, x2), smax(x3, x4)) || res < smin(smin(x1, x2), smin(x3, x4))) {
+      const double w = h * h;
+      res = w * x1;
+      res = madd(fma_, w, x2, res);
+      res = madd(fma_, w, x3, res);
+      res = madd(fma_, w, x4, res);
+    }
+    return res;
+  }
+  double part[6];
+  for (int c = 0; c < 6; ++c) {
+    double r = 0;
+    for (int q = 0; q < 36; ++q) {
+      double w = f[q % 6] * f[q / 6] * f[c];
+      double v = MS(q % 6 - 2, q / 6 - 2, c - 2);
+      r = q == 0 ? w * v : madd(fma_, w, v, r);
+    }
+    part[c] = r;
+  }
+  res = part[0];
+  for (int c = 1; c < 6; ++c) res = res + part[c];
+  /* max8 (:39-43) of x1 (0,0,0), x2 (1,0,0), x3 (0,1,0), x4 (0,0,1),
+   * x5 (1,1,0), x6 (1,0,1), x7 (0,1,1), x8 (1,1,1) */
+  double x[8] = {MS(0, 0, 0), MS(1, 0, 0), MS(0, 1, 0), MS(0, 0, 1),
+                 MS(1, 1, 0), MS(1, 0, 1), MS(0, 1, 1), MS(1, 1, 1)};
+  double mx = smax(smax(smax(x[0], x[1]), smax(x[2], x[3])), smax(smax(x[4], x[5]), smax(x[6], x[7])));
+  double mn = smin(smin(smin(x[0], x[1]), smin(x[2], x[3])), smin(smin(x[4], x[5]), smin(x[6], x[7])));
+  if (res > mx || res < mn) {
+    const double w = h * h * h;
+    /* :730-738: the z = 0 plane, then the z = 1 plane, each x fastest */
+    double r1 = w * x[0];
+    r1 = madd(fma_, w, x[1], r1);
+    r1 = madd(fma_, w, x[2], r1);
+    r1 = madd(fma_, w, x[4], r1);
+    double r2 = w * x[3];
+    r2 = madd(fma_, w, x[5], r2);
+    r2 = madd(fma_, w, x[6], r2);
+    r2 = madd(fma_, w, x[7], r2);
+    res = r1 + r2;
+  }
+  return res;
+#undef MS
+}
+
+int cgxo_prolongate_3d_o5_monotone_rf2(int fma_, const double *src, const int *srcpadext,
+                                       const int *srcext, double *dst, const int *dstpadext,
+                                       const int *dstext, const int *srcbbox_,
+                                       const int *dstbbox_, const int *srcregbbox_,
+                                       const int *regbbox_) {
+  (void)srcregbbox_; (void)dstext;
+  box_t srcbbox = mkbox(srcbbox_), dstbbox = mkbox(dstbbox_), reg = mkbox(regbbox_);
+  /* :72-86 */
+  for (int d = 0; d < 3; ++d) {
+    if (srcbbox.str[d] <= reg.str[d] || dstbbox.str[d] != reg.str[d])
+      return fail(CGXO_EINVAL, "prolongate_3d_o5_monotone_rf2: strides disagree");
+    if (srcbbox.str[d] != 2 * dstbbox.str[d])
+      return fail(CGXO_EINVAL, "prolongate_3d_o5_monotone_rf2: source strides are not twice the destination strides");
+  }
+  if (box_empty(&reg))
+    return fail(CGXO_EINVAL, "prolongate_3d_o5_monotone_rf2: region extent is empty");
+  /* :88-104 */
+  int regext[3], srcoff[3], dstoff[3], offlo[3], offhi[3];
+  for (int d = 0; d < 3; ++d) {
+    regext[d] = box_size(&reg, d);
+    if ((reg.lo[d] - srcbbox.lo[d]) % reg.str[d] || (reg.lo[d] - dstbbox.lo[d]) % reg.str[d])
+      return fail(CGXO_EINVAL, "prolongate_3d_o5_monotone_rf2: region not aligned");
+    srcoff[d] = (reg.lo[d] - srcbbox.lo[d]) / reg.str[d];
+    dstoff[d] = (reg.lo[d] - dstbbox.lo[d]) / reg.str[d];
+    offlo[d] = (srcoff[d] % 2 != 0 || regext[d] > 1) ? 3 : 0;
+    offhi[d] = ((srcoff[d] + regext[d] - 1) % 2 != 0 || regext[d] > 1) ? 3 : 0;
+  }
+  box_t ex = box_expand(&reg, offlo, offhi);
+  if (!box_in(&ex, &srcbbox) || !box_in(&reg, &dstbbox))
+    return fail(CGXO_EINVAL, "prolongate_3d_o5_monotone_rf2: region extent is not contained in array extent");
+  /* the coarse points actually read must be inside the source too: an odd
+   * fine point s reads s/2 - 2 .. s/2 + 3, an even one s/2 */
+  for (int d = 0; d < 3; ++d) {
+    int lo = 1 << 30, hi = -(1 << 30);
+    for (int s = srcoff[d]; s < srcoff[d] + regext[d] && s < srcoff[d] + 2; ++s) {
+      int a = s % 2 ? s / 2 - 2 : s / 2;
+      if (a < lo) lo = a;
+    }
+    for (int s = srcoff[d] + regext[d] - 1; s >= srcoff[d] && s > srcoff[d] + regext[d] - 3; --s) {
+      int a = s % 2 ? s / 2 + 3 : s / 2;
+      if (a > hi) hi = a;
+    }
+    if (lo < 0 || hi >= srcext[d])
+      return fail(CGXO_EINVAL, "prolongate_3d_o5_monotone_rf2: stencil reaches outside the source array");
+  }
+  for (int k = 0; k < regext[2]; ++k)
+    for (int j = 0; j < regext[1]; ++j)
+      for (int i = 0; i < regext[0]; ++i) {
+        const int s[3] = {srcoff[0] + i, srcoff[1] + j, srcoff[2] + k};
+        int b[3], ax[3], n = 0;
+        for (int d = 0; d < 3; ++d) {
+          b[d] = s[d] / 2;
+          if (s[d] % 2) ax[n++] = d;
+        }
+        dst[IDX(dstoff[0] + i, dstoff[1] + j, dstoff[2] + k, dstpadext)] =
+            mono_point(fma_, src, srcpadext, b, ax, n);
+      }
+  return CGXO_OK;
+}
+
+/* ------------------------------------------------------------------ */
 /* restrict_3d_rf2, CarpetLib/src/restrict_3d_rf2.cc:25-121             */
 
 int cgxo_restrict_3d_rf2(const double *src, const int *srcpadext,
@@ -1142,6 +1291,16 @@ static int transfer_p_r(int fma_, int op, int cent, double *dst,
         return cgxo_prolongate_3d_eno(fma_, src, srcpadext, srcext, dst, dstpadext,
                                       dstext, srcbbox, dstbbox, srcbox, dstbox);
       return fail(CGXO_EINVAL, "transfer_prolongate: no ENO stencil for this order");
+    }
+    if (op == op_Lagrange_monotone) {
+      /* data.cc:807-833: order 5 only, for every centring */
+      if (order_space == 1 || order_space == 3)
+        return fail(CGXO_EINVAL, "There is no stencil for op=\"Lagrange_monotone\" with order_space=%d",
+                    order_space);
+      if (order_space != 5)
+        return fail(CGXO_EINVAL, "There is no stencil for op=\"Lagrange_monotone\" with order_space!=5");
+      return cgxo_prolongate_3d_o5_monotone_rf2(fma_, src, srcpadext, srcext, dst, dstpadext,
+                                                dstext, srcbbox, dstbbox, srcbox, dstbox);
     }
     if (op == op_WENO) {
       /* data.cc:722-752: vertex-centred order 5 runs the ENO operator */

@@ -159,6 +159,11 @@ int cgxref_prolongate_3d_cc_eno_rf2(int order, OPARGS) {
   });
 }
 
+// prolongate_3d_o5_monotone_rf2 (CarpetLib/src/prolongate_3d_o5_monotone_rf2.cc:45)
+int cgxref_prolongate_3d_o5_monotone_rf2(OPARGS) {
+  return guarded([&] { call_operator(&prolongate_3d_o5_monotone_rf2<double>, OPCALL); });
+}
+
 // restrict_3d_rf2 (CarpetLib/src/restrict_3d_rf2.cc:25); called directly,
 // as CarpetLib/src/data.cc:1041 does through call_operator.
 int cgxref_restrict_3d_rf2(OPARGS) {

@@ -484,3 +484,49 @@ def test_transfer_high_order_time_and_restriction_in_time(port, order_time):
     d2 = r["dst"].copy()
     port.interpolate_3d_3tl(tmps, times[:3], r["reg"], d2, r["dstbbox"], r["reg"], t)
     assert bits_equal(d, d2)
+
+
+# ---------------------------------------------------------------- monotone order 5
+@needs_ref
+def test_o5_monotone_bit_exact_vs_reference(port):
+    """prolongate_3d_o5_monotone_rf2 (op Lagrange_monotone): the
+    tensor-product order-5 stencil with the min/max fallback"""
+    ref = Ref(False)
+    rng = np.random.default_rng(800)
+    for it in range(40):
+        kind = ("normal", "mixed", "steps", "smooth")[it % 4]
+        c = cases.vc_prolong_case(rng, 5, fine_stride=int(rng.choice([1, 2])), kind=kind)
+        d1, d2 = c["dst"].copy(), c["dst"].copy()
+        port.prolongate_3d_o5_monotone_rf2(c["src"], c["srcbbox"], d1, c["dstbbox"], c["reg"])
+        ref.prolongate_3d_o5_monotone_rf2(c["src"], c["srcbbox"], d2, c["dstbbox"], c["reg"])
+        assert bits_equal(d1, d2), (it, kind)
+
+
+def test_o5_monotone_selection_and_limiter(port):
+    """transfer's Lagrange_monotone entries (data.cc:807-833), and the
+    limiter: on smooth data the order-5 stencil, at jumps the fallback"""
+    from oracle.binding import OP_LAGRANGE_MONOTONE
+    rng = np.random.default_rng(810)
+    c = cases.vc_prolong_case(rng, 5, max_ext=10, kind="smooth")
+    want = c["dst"].copy()
+    port.prolongate_3d_o5_monotone_rf2(c["src"], c["srcbbox"], want, c["dstbbox"], c["reg"])
+    lag = c["dst"].copy()
+    port.prolongate_3d_rf2(5, c["src"], c["srcbbox"], lag, c["dstbbox"], c["reg"])
+    d = c["dst"].copy()
+    port.transfer(OP_LAGRANGE_MONOTONE, VERTEX, d, c["dstbbox"], [c["src"]], c["srcbbox"], [0.0],
+                  c["reg"], c["srcbbox"], 0.0, 5, 0)
+    assert bits_equal(d, want)
+    # smooth data: mostly the order-5 value, which agrees with Lagrange to rounding
+    r = cases.region_view(want, c["dstbbox"], c["reg"])
+    rl = cases.region_view(lag, c["dstbbox"], c["reg"])
+    assert np.mean(np.abs(r - rl) <= 1e-12 * (1 + np.abs(rl))) > 0.5
+    # piecewise-constant data: every value lies within its neighbours' range
+    s = cases.vc_prolong_case(rng, 5, max_ext=10, kind="steps")
+    d = s["dst"].copy()
+    port.prolongate_3d_o5_monotone_rf2(s["src"], s["srcbbox"], d, s["dstbbox"], s["reg"])
+    v = cases.region_view(d, s["dstbbox"], s["reg"])
+    assert v.min() >= s["src"].min() and v.max() <= s["src"].max()
+    for order, msg in ((1, "order_space=1"), (3, "order_space=3"), (7, "order_space!=5")):
+        with pytest.raises(OracleError, match=msg):
+            port.transfer(OP_LAGRANGE_MONOTONE, VERTEX, c["dst"].copy(), c["dstbbox"], [c["src"]],
+                          c["srcbbox"], [0.0], c["reg"], c["srcbbox"], 0.0, order, 0)
