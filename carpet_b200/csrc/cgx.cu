@@ -332,6 +332,46 @@ int build_spatial(int op, int cent, const cgx_array *dst, const cgx_array *src,
     if (slab) return fail(CGX_EINVAL, "transfer_p_r: slab with prolongation");
     const Box &reg = dstbox;
     int kind;
+    if (op == CGX_OP_LAGRANGE_MONOTONE) {
+      // data.cc:807-833, prolongate_3d_o5_monotone_rf2.cc:72-104 (any centring)
+      if (order_space == 1 || order_space == 3)
+        return fail(CGX_EINVAL, "There is no stencil for op=\"Lagrange_monotone\" with order_space=%d",
+                    order_space);
+      if (order_space != 5)
+        return fail(CGX_EINVAL, "There is no stencil for op=\"Lagrange_monotone\" with order_space!=5");
+      for (int k = 0; k < 3; ++k) {
+        if (sb.str[k] <= reg.str[k] || regdst.str[k] != reg.str[k])
+          return fail(CGX_EINVAL, "prolongate_3d_o5_monotone_rf2: strides disagree");
+        if (sb.str[k] != 2 * regdst.str[k])
+          return fail(CGX_EINVAL, "prolongate_3d_o5_monotone_rf2: source strides are not twice the "
+                                  "destination strides");
+      }
+      if (reg.empty()) return fail(CGX_EINVAL, "prolongate_3d_o5_monotone_rf2: region extent is empty");
+      Box ex = reg;
+      long long ncoarse = 1;
+      for (int k = 0; k < 3; ++k) {
+        if ((reg.lo[k] - sb.lo[k]) % reg.str[k] || (reg.lo[k] - regdst.lo[k]) % reg.str[k])
+          return fail(CGX_EINVAL, "prolongate_3d_o5_monotone_rf2: region not aligned");
+        d.n[k] = reg.size(k);
+        d.soff[k] = (reg.lo[k] - sb.lo[k]) / reg.str[k];
+        const int s0 = d.soff[k], s1 = s0 + d.n[k] - 1;
+        ex.lo[k] -= (s0 % 2 != 0 || d.n[k] > 1 ? 3 : 0) * reg.str[k];
+        ex.up[k] += (s1 % 2 != 0 || d.n[k] > 1 ? 3 : 0) * reg.str[k];
+        // coarse points read: s/2 for an even fine point s, s/2-2 .. s/2+3 for an odd one
+        const int cmin = d.n[k] > 1 || s0 % 2 ? s0 / 2 - 2 : s0 / 2;
+        const int cmax = d.n[k] > 1 || s1 % 2 ? (s1 - 1) / 2 + 3 : s1 / 2;
+        if (s0 < 0 || cmin < 0 || cmax >= sb.size(k))
+          return fail(CGX_EINVAL, "prolongate_3d_o5_monotone_rf2: stencil reaches outside the source array");
+        ncoarse *= cmax - cmin + 1;
+      }
+      if (!ex.in(sb) || !reg.in(regdst))
+        return fail(CGX_EINVAL, "prolongate_3d_o5_monotone_rf2: region extent is not contained in array extent");
+      d.kind = K_PROLONG_MONO;
+      d.order = 5;
+      out->points = reg.npoints();
+      out->bytes = 8 * out->points + 8 * ncoarse;
+      return CGX_OK;
+    }
     if (op == CGX_OP_COPY || op == CGX_OP_LAGRANGE) {
       if (cent == CGX_VERTEX) {
         if (order_space != 1 && order_space != 3 && order_space != 5 && order_space != 7 &&

@@ -29,7 +29,8 @@ enum Kind : int {
   K_RESTRICT_CC5 = 7, // restrict_3d_cc_o5_rf2 (6x6x6 cells, separable)
   K_PROLONG_CC_ENO = 8, // prolongate_3d_cc_eno_rf2<ORDER>, ORDER (d.order) 2 or 3
   K_TIME = 9,           // time_interpolate of per-timelevel temporaries
-  K_NKINDS = 10
+  K_PROLONG_MONO = 10,  // prolongate_3d_o5_monotone_rf2
+  K_NKINDS = 11
 };
 
 // T_LAG: interpolate_3d_4tl / interpolate_3d_5tl (ntl 4 or 5)
@@ -328,9 +329,13 @@ enum StreamVariant : int {
   SV_RESTRICT_CC = 5, // 8-point average
   SV_RESTRICT_CC3 = 6, // third-order cell-centred restriction
   SV_RESTRICT_CC5 = 7, // fifth-order cell-centred restriction
-  SV_TIME = 8,         // time combination of temporaries (K_TIME)
-  SV_COUNT = 9
+  SV_MONO = 8,         // monotone order-5 prolongation
+  SV_TIME = 9,         // time combination of temporaries (K_TIME)
+  SV_COUNT = 10
 };
+// A batch launches its segments in order: the time combination of staged
+// transfers must come after every kind that writes their temporaries.
+static_assert(SV_TIME == SV_COUNT - 1, "the time combination is the last streaming variant");
 
 template <class D> __host__ __device__ __forceinline__ int stream_variant(const D &d) {
   if (d.kind == K_RESTRICT_VC) return SV_RESTRICT_VC;
@@ -338,6 +343,7 @@ template <class D> __host__ __device__ __forceinline__ int stream_variant(const 
   if (d.kind == K_RESTRICT_CC3) return SV_RESTRICT_CC3;
   if (d.kind == K_RESTRICT_CC5) return SV_RESTRICT_CC5;
   if (d.kind == K_TIME) return SV_TIME;
+  if (d.kind == K_PROLONG_MONO) return SV_MONO;
   if (d.kind != K_COPY) return -1;
   if (d.ntl == 1) return SV_COPY1;
   if (d.ntl == 2) return SV_COPY2;
@@ -503,6 +509,113 @@ __device__ __forceinline__ void time_tile(const D &d, int tile, int lid) {
     int i, j, k;
     unflatten(d, p, i, j, k);
     dst[i + j * d.dsy + k * d.dsz] = res;
+  }
+}
+
+// prolongate_3d_o5_monotone_rf2 (prolongate_3d_o5_monotone_rf2.cc:45-793),
+// one fine point per lane.  q points at the coarse base; odd axes take the
+// tensor-product order-5 stencil over coarse -2 .. +3, summed left to right
+// with the lowest odd axis fastest (weights f_a * f_b * f_c formed left to
+// right); with three odd axes every z plane is a partial sum of its own and
+// the six are added in order (:499-716).  A result outside the nearest 2/4/8
+// coarse values (std::min/std::max nested as min4/max4/min8/max8, :19-43)
+// falls back to linear, bilinear or trilinear interpolation.
+__device__ __forceinline__ double smin(double a, double b) { return b < a ? b : a; }
+__device__ __forceinline__ double smax(double a, double b) { return a < b ? b : a; }
+__device__ __forceinline__ constexpr double mono_f(int m) {
+  return (m == 0 || m == 5 ? 3.0 : m == 1 || m == 4 ? -25.0 : 150.0) / 256;
+}
+template <int FMA>
+__device__ __forceinline__ double mono_point(const double *q, int ox, int oy, int oz, long long sy,
+                                             long long sz) {
+  const int n = ox + oy + oz;
+  if (n == 0) return __ldg(q);
+  if (n == 1) {
+    const long long s = ox ? 1 : oy ? sy : sz;
+    double res = mul(mono_f(0), __ldg(q - 2 * s));
+#pragma unroll
+    for (int m = 1; m < 6; ++m) res = madd<FMA>(mono_f(m), __ldg(q + (m - 2) * s), res);
+    const double v0 = __ldg(q), v1 = __ldg(q + s);
+    if (res > smax(v0, v1) || res < smin(v0, v1)) res = madd<FMA>(0.5, v1, mul(0.5, v0));
+    return res;
+  }
+  if (n == 2) {
+    const long long s0 = ox ? 1 : sy, s1 = oz ? sz : sy;
+    double res = 0.0;
+#pragma unroll
+    for (int b = 0; b < 6; ++b) {
+      const double *row = q + (b - 2) * s1 - 2 * s0;
+#pragma unroll
+      for (int a = 0; a < 6; ++a) {
+        const double w = mono_f(a) * mono_f(b);
+        const double v = __ldg(row + a * s0);
+        res = (a == 0 && b == 0) ? mul(w, v) : madd<FMA>(w, v, res);
+      }
+    }
+    const double x1 = __ldg(q), x2 = __ldg(q + s0), x3 = __ldg(q + s1), x4 = __ldg(q + s0 + s1);
+    if (res > smax(smax(x1, x2), smax(x3, x4)) || res < smin(smin(x1, x2), smin(x3, x4))) {
+      res = mul(0.25, x1);
+      res = madd<FMA>(0.25, x2, res);
+      res = madd<FMA>(0.25, x3, res);
+      res = madd<FMA>(0.25, x4, res);
+    }
+    return res;
+  }
+  double res = 0.0;
+#pragma unroll 1
+  for (int c = 0; c < 6; ++c) {
+    const double fc = (c == 0 || c == 5) ? mono_f(0) : (c == 1 || c == 4) ? mono_f(1) : mono_f(2);
+    const double *pl = q + (c - 2) * sz;
+    double r = 0.0;
+#pragma unroll
+    for (int b = 0; b < 6; ++b) {
+      const double *row = pl + (b - 2) * sy - 2;
+#pragma unroll
+      for (int a = 0; a < 6; ++a) {
+        const double w = __dmul_rn(mono_f(a) * mono_f(b), fc);
+        const double v = __ldg(row + a);
+        r = (a == 0 && b == 0) ? mul(w, v) : madd<FMA>(w, v, r);
+      }
+    }
+    res = c == 0 ? r : add(res, r);
+  }
+  // max8 / min8 of (0,0,0), (1,0,0), (0,1,0), (0,0,1), (1,1,0), (1,0,1), (0,1,1), (1,1,1)
+  const double x0 = __ldg(q), x1 = __ldg(q + 1), x2 = __ldg(q + sy), x3 = __ldg(q + sz);
+  const double x4 = __ldg(q + 1 + sy), x5 = __ldg(q + 1 + sz), x6 = __ldg(q + sy + sz);
+  const double x7 = __ldg(q + 1 + sy + sz);
+  const double mx = smax(smax(smax(x0, x1), smax(x2, x3)), smax(smax(x4, x5), smax(x6, x7)));
+  const double mn = smin(smin(smin(x0, x1), smin(x2, x3)), smin(smin(x4, x5), smin(x6, x7)));
+  if (res > mx || res < mn) {
+    // :730-738: the z = 0 plane, then the z = 1 plane, x fastest
+    double r1 = mul(0.125, x0);
+    r1 = madd<FMA>(0.125, x1, r1);
+    r1 = madd<FMA>(0.125, x2, r1);
+    r1 = madd<FMA>(0.125, x4, r1);
+    double r2 = mul(0.125, x3);
+    r2 = madd<FMA>(0.125, x5, r2);
+    r2 = madd<FMA>(0.125, x6, r2);
+    r2 = madd<FMA>(0.125, x7, r2);
+    res = add(r1, r2);
+  }
+  return res;
+}
+
+template <int FMA, int LANES, class D>
+__device__ __forceinline__ void mono_tile(const D &d, int tile, int lid) {
+  constexpr int PER = STILE / LANES;
+  const unsigned npts = (unsigned)d.n[0] * d.n[1] * d.n[2];
+  const unsigned p0 = (unsigned)tile * STILE + lid;
+  const long long sy = d.ssy, sz = d.ssz;
+  double *dst = d.dst + (d.doff[0] + d.doff[1] * d.dsy + d.doff[2] * d.dsz);
+#pragma unroll 1
+  for (int r = 0; r < PER; ++r) {
+    const unsigned p = p0 + r * LANES;
+    if (p >= npts) break;
+    int i, j, k;
+    unflatten(d, p, i, j, k);
+    const int fx = d.soff[0] + i, fy = d.soff[1] + j, fz = d.soff[2] + k;
+    const double *q = d.src[0] + ((fx >> 1) + (fy >> 1) * sy + (long long)(fz >> 1) * sz);
+    dst[i + j * d.dsy + k * d.dsz] = mono_point<FMA>(q, fx & 1, fy & 1, fz & 1, sy, sz);
   }
 }
 

@@ -141,6 +141,8 @@ int launch_stream_map_t(int variant, const Desc *d_descs, const int2 *d_tmap, lo
     return launch_stream_v<FMA, SV_RESTRICT_CC5>(d_descs, d_tmap, ntiles, d_counter, d_status, s);
   case SV_TIME:
     return launch_stream_v<FMA, SV_TIME>(d_descs, d_tmap, ntiles, d_counter, d_status, s);
+  case SV_MONO:
+    return launch_stream_v<FMA, SV_MONO>(d_descs, d_tmap, ntiles, d_counter, d_status, s);
   }
   return set_error(CGX_EINVAL, "bad streaming variant %d", variant);
 }

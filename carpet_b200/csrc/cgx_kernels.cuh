@@ -225,7 +225,8 @@ __device__ __forceinline__ void stream_tile(const Desc &d, int tile, int lid) {
   else if (V == SV_RESTRICT_CC) restrict_cc_tile<FMA, LANES>(d, tile, lid);
   else if (V == SV_RESTRICT_CC3) restrict_cc3_tile<FMA, LANES>(d, tile, lid);
   else if (V == SV_RESTRICT_CC5) restrict_cc5_tile<FMA, LANES>(d, tile, lid);
-  else time_tile<FMA, LANES>(d, tile, lid);
+  else if (V == SV_TIME) time_tile<FMA, LANES>(d, tile, lid);
+  else mono_tile<FMA, LANES>(d, tile, lid);
 }
 
 // Per-box form: a CTA per tile, every variant in one dispatch.  The
@@ -248,6 +249,7 @@ __global__ void __launch_bounds__(NTHREADS, STREAM_BLOCKS_PER_SM)
   case SV_RESTRICT_CC3: stream_tile<FMA, SV_RESTRICT_CC3, NTHREADS>(s_d, t, l); return;
   case SV_RESTRICT_CC5: stream_tile<FMA, SV_RESTRICT_CC5, NTHREADS>(s_d, t, l); return;
   case SV_TIME: stream_tile<FMA, SV_TIME, NTHREADS>(s_d, t, l); return;
+  case SV_MONO: stream_tile<FMA, SV_MONO, NTHREADS>(s_d, t, l); return;
   }
   if (threadIdx.x == 0) report(status, CGX_EDEVICE);
 }

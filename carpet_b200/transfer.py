@@ -23,7 +23,8 @@ from . import _lib
 from ._lib import CgxError, box9, check, cgx_array, ints3, lib
 
 # operator_type (CarpetLib/src/operators.hh:8-25), centering (defs.hh:134)
-OP_ERROR, OP_NONE, OP_SYNC, OP_RESTRICT, OP_COPY, OP_LAGRANGE, OP_ENO, OP_WENO = range(8)
+OP_ERROR, OP_NONE, OP_SYNC, OP_RESTRICT, OP_COPY, OP_LAGRANGE, OP_ENO, OP_WENO, OP_TVD, \
+    OP_LAGRANGE_MONOTONE = range(10)
 VERTEX, CELL = 1, 2
 
 

@@ -12,7 +12,8 @@ import numpy as np
 import pytest
 
 from oracle import cases
-from oracle.binding import OP_COPY, OP_ENO, OP_LAGRANGE, OP_WENO, CELL, VERTEX, OracleError, alloc
+from oracle.binding import (OP_COPY, OP_ENO, OP_LAGRANGE, OP_LAGRANGE_MONOTONE, OP_WENO, CELL,
+                            VERTEX, OracleError, alloc)
 
 pytestmark = pytest.mark.gpu
 
@@ -120,6 +121,21 @@ def test_vc_eno(cgx, port, ntl, fma, form):
         c = cases.vc_prolong_case(rng, 3, reach=(1, 2), max_ext=40 if it == 7 else 9,
                                   kind=("normal", "steps", "mixed")[it % 3])
         got, want = run_pair(cgx, port, c, OP_ENO, VERTEX, 3, ntl, fma, rng, form)
+        assert bits_equal(got, want)
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("fma", [False, True], ids=["exact", "fma"])
+@pytest.mark.parametrize("ntl", [1, 2, 3])
+def test_o5_monotone(cgx, port, ntl, fma, form):
+    """op Lagrange_monotone: prolongate_3d_o5_monotone_rf2, with ENO time
+    interpolation through temporaries for 2 and 3 timelevels"""
+    rng = np.random.default_rng(3200 + ntl)
+    for it in range(6):
+        c = cases.vc_prolong_case(rng, 5, fine_stride=int(rng.choice([1, 2])),
+                                  max_ext=30 if it == 5 else 9,
+                                  kind=("normal", "mixed", "steps", "smooth")[it % 4])
+        got, want = run_pair(cgx, port, c, OP_LAGRANGE_MONOTONE, VERTEX, 5, ntl, fma, rng, form)
         assert bits_equal(got, want)
 
 
@@ -346,6 +362,8 @@ def staged_cases(rng, big=False):
         out.append((cases.vc_restrict_case(rng, max_ext=m, kind="mixed"), OP_LAGRANGE, VERTEX, 1, ntl))
         out.append((cases.cc_restrict_case(rng, max_ext=m, kind="mixed"), OP_LAGRANGE, CELL, 1, ntl))
         out.append((cases.cc_restrict_case(rng, max_ext=m, kind="mixed"), OP_ENO, CELL, 1, ntl))
+        out.append((cases.vc_prolong_case(rng, 5, max_ext=m, kind="steps"), OP_LAGRANGE_MONOTONE,
+                    VERTEX, 5, ntl))
     return out
 
 
