@@ -629,19 +629,22 @@ def main():
                  "ms_per_step": round(pms, 3), "launches_per_step": stats[0]["pairs"]}
 
     # end to end: grid data in pinned host memory; every step copies in all
-    # it reads and copies out all it writes (whole levels per timelevel).
-    # Two device copies of the hierarchy alternate, so that a step's copy-in
-    # overlaps the previous step's transfers and copy-out (the two copy
-    # directions and the kernels run on three streams).
+    # it reads and copies out all it writes: every timelevel of every level,
+    # since one coarse step rotates the finer levels through all their
+    # timelevels (each substep writes ghost zones and boundary shells of its
+    # current one).  Two device copies of the hierarchy alternate, so that a
+    # step's copy-in overlaps the previous step's transfers and copy-out (the
+    # two copy directions and the kernels run on three streams).
     e2e = None
     if not args.no_e2e:
         host = [[torch.empty_like(p, device="cpu").pin_memory() for p in lp] for lp in st.pools]
         for lp, hp in zip(st.pools, host):
             for p, q in zip(lp, hp):
                 q.copy_(p)
-        hout = [[torch.empty_like(lp[0], device="cpu").pin_memory() for lp in st.pools] for _ in range(2)]
+        # one set of output buffers: the copy-out stream writes them in step order
+        hout = [[torch.empty_like(p, device="cpu").pin_memory() for p in lp] for lp in st.pools]
         h2d = sum(p.numel() * 8 for lp in st.pools for p in lp)
-        d2h = sum(lp[0].numel() * 8 for lp in st.pools)
+        d2h = h2d
         stB = Storage(h, args.ngf, 3)
         for la, lb in zip(st.pools, stB.pools):
             for p, q in zip(la, lb):
@@ -670,7 +673,7 @@ def main():
 
         def e2e_step(s):
             x = s % 2
-            sto, bx, gr = bufs[x]
+            sto, _, gr = bufs[x]
             if used[x]:
                 s_in.wait_event(out_done[x])  # the buffer's last step is copied out
             with torch.cuda.stream(s_in):
@@ -683,8 +686,9 @@ def main():
             comp_done[x].record(stream)
             s_out.wait_event(comp_done[x])
             with torch.cuda.stream(s_out):
-                for l, lp in enumerate(sto.pools):
-                    hout[x][l].copy_(lp[bx.pool_index(bx.rot[l], 0)], non_blocking=True)
+                for lp, hp in zip(sto.pools, hout):
+                    for p, q in zip(lp, hp):
+                        q.copy_(p, non_blocking=True)
             out_done[x].record(s_out)
             used[x] = True
 
