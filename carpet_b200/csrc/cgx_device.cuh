@@ -317,7 +317,7 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 // CTA: every lane is busy whatever the shape, consecutive lanes touch
 // consecutive x, and each thread issues a group of loads before its stores.  A flat index is split into (i, j, k) by
 // 32-bit multiply-high with precomputed magic numbers.
-constexpr int STILE = 2048;
+constexpr int STILE = 1024;
 
 // The streaming kinds, one persistent kernel each.
 enum StreamVariant : int {

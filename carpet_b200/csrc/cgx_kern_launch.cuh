@@ -20,11 +20,12 @@ template <int FMA, bool HIGH> int launch_pair_t(const Desc &d, int ntiles, int *
 }
 
 // grid of a persistent kernel: every CTA slot of the device, at most ntiles
-template <class K> int persistent_grid(K kernel, size_t smem, long long ntiles, int *grid) {
+template <class K>
+int persistent_grid(K kernel, size_t smem, long long ntiles, int *grid, int threads = NTHREADS) {
   int dev = 0, nsm = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, NTHREADS, smem);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
   if (e != cudaSuccess || per_sm < 1) per_sm = 1;
   *grid = (int)std::min<long long>((long long)nsm * per_sm, ntiles);
   return CGX_OK;
@@ -117,8 +118,8 @@ template <int FMA, int V>
 int launch_stream_v(const Desc *d_descs, const int2 *d_tmap, long long ntiles,
                     unsigned long long *d_counter, int *d_status, cudaStream_t s) {
   int grid = 0;
-  persistent_grid(k_stream_map<FMA, V>, 0, ntiles, &grid);
-  k_stream_map<FMA, V><<<grid, NTHREADS, 0, s>>>(d_descs, d_tmap, ntiles, d_counter, d_status);
+  persistent_grid(k_stream_map<FMA, V>, 0, ntiles, &grid, STREAM_THREADS);
+  k_stream_map<FMA, V><<<grid, STREAM_THREADS, 0, s>>>(d_descs, d_tmap, ntiles, d_counter, d_status);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? CGX_OK : cuda_error(e, "k_stream_map launch");
 }

@@ -212,6 +212,8 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 // Streaming kernels (copy and restrictions): no shared-memory stage, so
 // they run at high occupancy -- many warps keep their loads in flight.
 constexpr int STREAM_BLOCKS_PER_SM = 4;
+// the persistent streaming kernels: smaller CTAs, more of them per SM
+constexpr int STREAM_THREADS = 128, STREAM_MAP_BLOCKS_PER_SM = 8;
 
 // one streaming variant's tile, run by LANES threads (lid: 0 .. LANES-1);
 // V is a StreamVariant
@@ -260,7 +262,7 @@ __global__ void __launch_bounds__(NTHREADS, STREAM_BLOCKS_PER_SM)
 // tile's descriptor into the second of two shared buffers while the current
 // tile runs.
 template <int FMA, int V>
-__global__ void __launch_bounds__(NTHREADS, STREAM_BLOCKS_PER_SM)
+__global__ void __launch_bounds__(STREAM_THREADS, STREAM_MAP_BLOCKS_PER_SM)
     k_stream_map(const Desc *__restrict__ descs, const int2 *__restrict__ tmap, long long ntiles,
                  unsigned long long *counter, int *status) {
   __shared__ __align__(16) Desc s_d[2];
@@ -291,7 +293,7 @@ __global__ void __launch_bounds__(NTHREADS, STREAM_BLOCKS_PER_SM)
     const int tile = s_m[slot].y;
     if (tid == 0) claim((i + 2) % 3);
     stage(buf ^ 1, (i + 1) % 3);
-    if (stream_variant(s_d[buf]) == V) stream_tile<FMA, V, NTHREADS>(s_d[buf], tile, tid);
+    if (stream_variant(s_d[buf]) == V) stream_tile<FMA, V, STREAM_THREADS>(s_d[buf], tile, tid);
     else if (tid == 0) report(status, CGX_EDEVICE);
     __syncthreads();
   }
