@@ -1,0 +1,167 @@
+"""Full-size checks on the benchmark workload: 5 vertex-centred levels of
+129^3 points, each split into 2x2x2 components, 3 timelevels, ghost 3,
+buffer 9, order-5 Lagrange prolongation with quadratic time interpolation,
+injection and ghost sync -- one coarse Berger-Oliger step, FMA mode.
+
+* the whole step on the device for every grid function, and the oracle's
+  replay of the same phases for a sample of grid functions (grid functions
+  never mix, so each is a full-size parity case): bit-exact;
+* a separable cubic field is reproduced exactly by every operator on the
+  path (Lagrange of order 5 holds cubics, the time weights of equal
+  timelevels sum to one, and every intermediate value is an exactly
+  representable integer multiple of a power of two), so two whole steps
+  leave every point of every array bit-identical;
+* the batched kernels (TMA-staged prolongation, persistent streaming
+  kernels) and the per-box kernels (cp.async-staged prolongation, per-box
+  streaming) give the same bits on the whole step.
+"""
+import numpy as np
+import pytest
+
+from oracle.binding import OP_LAGRANGE, VERTEX
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+LEVELS, NPOINTS = 5, 129
+
+
+@pytest.fixture(scope="module")
+def cgx():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import carpet_b200 as cb
+    return cb
+
+
+def workload(cb, ngf, fill):
+    from carpet_b200.amr import BergerOliger, Storage
+    from carpet_b200.hierarchy import nested
+    cb.set_fp_mode(True)
+    h = nested(LEVELS, NPOINTS, ghost=3, buffer=9, order=5)
+    st = Storage(h, ngf, 3)
+    fill(st, h)
+    bo = BergerOliger(h, st, order_space=5, order_time=2)
+    return h, st, bo
+
+
+def random_fill(st, h):
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(7)
+    for lp in st.pools:
+        for p in lp:
+            p.normal_(generator=gen)
+
+
+def cubic_fill(st, h):
+    """p(x) + q(y) + r(z), cubics with small integer coefficients in the
+    global integer coordinates (at most 2048): values below 2^36; the same
+    on every timelevel, different on every grid function"""
+    for l, lev in enumerate(h.levels):
+        for tl in range(st.ntl):
+            for g in range(st.ngf):
+                for c, comp in enumerate(lev.comps):
+                    b = comp.exterior
+                    t = st.data[l][tl][g][c].tensor
+                    nz, ny = t.shape[0], t.shape[1]
+                    nx = (b[3] - b[0]) // b[6] + 1
+                    x = (b[0] + torch.arange(nx, device="cuda", dtype=torch.float64) * b[6])
+                    y = (b[1] + torch.arange(ny, device="cuda", dtype=torch.float64) * b[7])
+                    z = (b[2] + torch.arange(nz, device="cuda", dtype=torch.float64) * b[8])
+                    px = 2 * x ** 3 - 3 * x ** 2 + x + g
+                    qy = y ** 3 + 5 * y ** 2 - 7 * y
+                    rz = -z ** 3 + 2 * z ** 2 + 3 * z
+                    t[:, :, :nx] = rz[:, None, None] + qy[None, :, None] + px[None, None, :]
+
+
+def host_copy(st, gfs):
+    return {g: [[[st.data[l][p][g][c].tensor.cpu().numpy().copy()
+                  for c in range(len(st.data[l][p][g]))] for p in range(st.ntl)]
+                for l in range(len(st.data))] for g in gfs}
+
+
+def oracle_phase(port, h, arr, key):
+    """one phase of BergerOliger on one grid function's host arrays
+    arr[level][pool][comp], in the batches' own terms (carpet_b200.amr)"""
+    kind, l, rots, ntl = key
+    pool = lambda r, tl: (tl - r) % 3
+    ext = lambda lv, c: list(h.levels[lv].comps[c].exterior)
+    if kind == "sync":
+        r, = rots
+        a = arr[l][pool(r, 0)]
+        for p in h.sync[l]:
+            port.transfer(OP_LAGRANGE, VERTEX, a[p.dst_comp], ext(l, p.dst_comp), [a[p.src_comp]],
+                          ext(l, p.src_comp), [0.0], list(p.dstbox), list(p.srcbox), 0.0, 1, 0,
+                          fma=True)
+    elif kind == "prolong":
+        rf, rc = rots
+        dst = arr[l][pool(rf, 0)]
+        srcs = [arr[l - 1][pool(rc, t)] for t in range(3)]
+        dtc = 1.0 / 64
+        times, time = [0.0, -dtc, -2 * dtc], (-dtc / 2 if ntl > 1 else 0.0)
+        for p in h.prolong[l]:
+            port.transfer(OP_LAGRANGE, VERTEX, dst[p.dst_comp], ext(l, p.dst_comp),
+                          [s[p.src_comp] for s in srcs], ext(l - 1, p.src_comp), times,
+                          list(p.dstbox), list(p.srcbox), time, 5, 2, fma=True)
+    else:
+        rc, rf = rots
+        dst, src = arr[l][pool(rc, 0)], arr[l + 1][pool(rf, 0)]
+        for p in h.restrict[l + 1]:
+            port.transfer(OP_LAGRANGE, VERTEX, dst[p.dst_comp], ext(l, p.dst_comp),
+                          [src[p.src_comp]], ext(l + 1, p.src_comp), [0.0], list(p.dstbox),
+                          list(p.srcbox), 0.0, 5, 0, fma=True)
+
+
+def test_bench_step_matches_oracle_on_sampled_grid_functions(cgx, port):
+    ngf = 25
+    h, st, bo = workload(cgx, ngf, random_fill)
+    gfs = (0, ngf - 1)
+    want = host_copy(st, gfs)
+    keys = bo.step_phases()
+    bo.run(keys)
+    for b in bo.batches.values():
+        b.check()
+    torch.cuda.synchronize()
+    got = host_copy(st, gfs)
+    for g in gfs:
+        for k in keys:
+            oracle_phase(port, h, want[g], k)
+        for l in range(LEVELS):
+            for p in range(3):
+                for c, a in enumerate(want[g][l][p]):
+                    assert np.array_equal(a.view(np.uint64), got[g][l][p][c].view(np.uint64)), \
+                        ("grid function", g, "level", l, "pool", p, "component", c)
+
+
+def test_cubic_field_survives_two_steps_bit_exact(cgx):
+    h, st, bo = workload(cgx, 4, cubic_fill)
+    before = [[p.clone() for p in lp] for lp in st.pools]
+    for _ in range(2):
+        keys = bo.step_phases()
+        bo.run(keys)
+    for b in bo.batches.values():
+        b.check()
+    torch.cuda.synchronize()
+    for l, (lp, bp) in enumerate(zip(st.pools, before)):
+        for p, q in zip(lp, bp):
+            assert torch.equal(p.view(torch.int64), q.view(torch.int64)), ("level", l)
+
+
+def test_batched_and_per_box_kernels_agree_on_the_step(cgx):
+    h, st, bo = workload(cgx, 4, random_fill)
+    init = [[p.clone() for p in lp] for lp in st.pools]
+    keys = bo.step_phases()
+    bo.run(keys)
+    torch.cuda.synchronize()
+    batched = [[p.clone() for p in lp] for lp in st.pools]
+    for lp, ip in zip(st.pools, init):
+        for p, q in zip(lp, ip):
+            p.copy_(q)
+    bo.run(keys, per_box=True)
+    for b in bo.batches.values():
+        b.check()
+    torch.cuda.synchronize()
+    for l, (lp, bp) in enumerate(zip(st.pools, batched)):
+        for p, q in zip(lp, bp):
+            assert torch.equal(p.view(torch.int64), q.view(torch.int64)), ("level", l)
