@@ -90,7 +90,16 @@ const char *cgx_version(void);
  * (transfer_prolongate data.cc:573-725, transfer_restrict data.cc:1030-1135,
  * time_interpolate data.cc:1183-1299), same argument checks as status codes.
  * The spatial operator and the time interpolation run fused in one kernel,
- * in the reference's order (space per timelevel, then time).
+ * in the reference's order (space per timelevel, then time), for copies and
+ * prolongations with up to 3 timelevels.  Restriction between timelevels and
+ * 4 or 5 timelevels (interpolate_3d_4tl / 5tl) run the reference's two
+ * stages: per-timelevel temporaries (stream-ordered allocation), then the
+ * time combination.
+ * Operators: vertex-centred Lagrange 1-11, cell-centred Lagrange 0-5,
+ * vertex-centred ENO 3/5 and WENO 5 (the ENO operator), cell-centred ENO 2-5,
+ * Lagrange_monotone 5, injection, cell-centred restriction (orders 1/3/5 by
+ * cgx_set_restriction), copy with slab offset; other operators return
+ * CGX_EUNSUPPORTED.
  *   srcs[nsrc], times[nsrc]: source timelevels (same padext/bbox each);
  *   slab_offset: NULL or int[3], the islab offset of copy_3d (copy_3d.cc:57);
  *   stream: a cudaStream_t (NULL = default stream).
