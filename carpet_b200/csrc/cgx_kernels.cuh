@@ -53,6 +53,9 @@ template <int FMA> __device__ __noinline__ void restrict_cc3_entry(const Desc &d
 template <int FMA> __device__ __noinline__ void restrict_cc5_entry(const Desc &d, int tile) {
   restrict_cc5_tile<FMA, NTHREADS>(d, tile, threadIdx.x);
 }
+template <int FMA> __device__ __noinline__ void mono_entry(const Desc &d, int tile) {
+  mono_tile<FMA, NTHREADS>(d, tile, threadIdx.x);
+}
 
 template <class F, int FMA>
 __device__ __forceinline__ void prolong_ntl(const Desc &d, int tile, double *sm) {
@@ -81,6 +84,7 @@ __device__ __forceinline__ void run_tile(const Desc &d, int tile, double *sm, in
   case K_RESTRICT_CC: restrict_cc_entry<FMA>(d, tile); return;
   case K_RESTRICT_CC3: restrict_cc3_entry<FMA>(d, tile); return;
   case K_RESTRICT_CC5: restrict_cc5_entry<FMA>(d, tile); return;
+  case K_PROLONG_MONO: mono_entry<FMA>(d, tile); return;
   case K_PROLONG_VC:
     if (HIGH) {
       switch (d.order) {

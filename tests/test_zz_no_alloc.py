@@ -20,7 +20,7 @@ import numpy as np
 import pytest
 
 from oracle import cases
-from oracle.binding import CELL, OP_ENO, OP_LAGRANGE, VERTEX
+from oracle.binding import CELL, OP_ENO, OP_LAGRANGE, OP_LAGRANGE_MONOTONE, VERTEX
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
@@ -43,7 +43,7 @@ def _make_pairs(seed, n):
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n):
-        k = i % 6
+        k = i % 8
         if k == 0:
             order = int(rng.choice([1, 3, 5]))
             out.append((OP_LAGRANGE, VERTEX, cases.vc_prolong_case(rng, order, max_ext=30), order))
@@ -56,8 +56,12 @@ def _make_pairs(seed, n):
             out.append((OP_LAGRANGE, VERTEX, cases.vc_restrict_case(rng, max_ext=24), 1))
         elif k == 4:
             out.append((OP_LAGRANGE, CELL, cases.cc_restrict_case(rng, max_ext=24), 0))
-        else:
+        elif k == 5:
             out.append((OP_LAGRANGE, VERTEX, cases.copy_case(rng, max_ext=30), 1))
+        elif k == 6:
+            out.append((OP_LAGRANGE_MONOTONE, VERTEX, cases.vc_prolong_case(rng, 5, max_ext=20), 5))
+        else:
+            out.append((OP_ENO, CELL, cases.cc_prolong_case(rng, 5, max_ext=20, kind="smooth"), 5))
     return out
 
 
@@ -78,7 +82,9 @@ def _run(lib, seed, n):
     t0, dt = 0.5, 0.125
     for i, (op, cent, c, order) in enumerate(_make_pairs(seed, n)):
         ntl = 1 + i % 3
-        if c["srcbbox"][6] < c["dstbbox"][6]:  # restriction: one timelevel
+        # restriction, and the monotone operator (between timelevels it runs
+        # through temporaries, which this entry point does not allocate)
+        if c["srcbbox"][6] < c["dstbbox"][6] or op == OP_LAGRANGE_MONOTONE:
             ntl = 1
         times = [t0, t0 - dt, t0 - 2 * dt]
         time = t0 if ntl == 1 else t0 - dt / (3 if ntl == 2 else 2)
@@ -154,3 +160,38 @@ def test_noalloc_rejects_too_many_pairs(lib):
     rc = lib.cgx_transfer_pairs_noalloc(pairs, n, None)
     assert rc == 1
     assert b"2048" in lib.cgx_last_error()
+
+
+def test_noalloc_refuses_pairs_that_need_temporaries(lib):
+    """a restriction between timelevels runs through per-timelevel
+    temporaries, which this entry point does not allocate"""
+    from carpet_b200._lib import box9  # noqa: F401  (loads the library)
+    cgx_array, cgx_pair = _structs()
+    rng = np.random.default_rng(779)
+    c = cases.vc_restrict_case(rng, max_ext=8)
+    src = torch.from_numpy(c["src"].copy()).cuda()
+    dst = torch.from_numpy(c["dst"].copy()).cuda()
+
+    def arr(t, bbox):
+        a = cgx_array()
+        a.data = t.data_ptr()
+        a.padext[:] = (t.shape[2], t.shape[1], t.shape[0])
+        a.bbox[:] = bbox
+        return a
+
+    pairs = (cgx_pair * 1)()
+    p = pairs[0]
+    p.op, p.cent = OP_LAGRANGE, VERTEX
+    p.dst = arr(dst, c["dstbbox"])
+    for t in range(3):
+        p.srcs[t] = arr(src, c["srcbbox"])
+    p.times[:] = [0.5, 0.375, 0.25]
+    p.nsrc = 3
+    p.dstbox[:] = c["reg"]
+    p.srcbox[:] = c["srcbbox"]
+    p.has_slab = 0
+    p.time = 0.45
+    p.order_space, p.order_time = 1, 2
+    rc = lib.cgx_transfer_pairs_noalloc(pairs, 1, None)
+    assert rc == 2, lib.cgx_last_error()
+    assert b"temporaries" in lib.cgx_last_error()
