@@ -875,7 +875,10 @@ int cgx_copy(int op, int cent, const cgx_array *dst, const cgx_array *src, const
 int cgx_batch_create(cgx_batch **out) {
   if (!out) return fail(CGX_EINVAL, "null batch");
   cgx_batch *b = new cgx_batch();
-  cudaError_t e = cudaMalloc(&b->d_counter, NSEG * sizeof(unsigned long long));
+  // per segment a claim counter and, NSEG further, an exit count (the
+  // kernels reset both when they finish)
+  cudaError_t e = cudaMalloc(&b->d_counter, 2 * NSEG * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(b->d_counter, 0, 2 * NSEG * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMalloc(&b->d_status, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(b->d_status, 0, sizeof(int));
   if (e != cudaSuccess) {
@@ -1066,8 +1069,8 @@ int cgx_batch_launch(cgx_batch *b, void *stream) {
     if (rc) return rc;
   }
   if (b->n_uploaded > 0) {
-    cudaError_t e = cudaMemsetAsync(b->d_counter, 0, NSEG * sizeof(unsigned long long), s);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    // the segment kernels leave their counters at zero: no memset between
+    // the launches, which run chained
     int rc = launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, b->seg, b->tma_cfg, b->d_counter,
                         b->d_status, s);
     if (rc) return rc;
@@ -1178,7 +1181,9 @@ int cgx_batch_check(cgx_batch *b, void *stream) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "status read");
   if (st) {
+    // a kernel that gave up may have left its counters behind
     cudaMemsetAsync(b->d_status, 0, sizeof(int), s);
+    cudaMemsetAsync(b->d_counter, 0, 2 * NSEG * sizeof(unsigned long long), s);
     return fail(st, "a kernel reported status %d", st);
   }
   return CGX_OK;

@@ -20,6 +20,25 @@ template <int FMA, bool HIGH> int launch_pair_t(const Desc &d, int ntiles, int *
 }
 
 // grid of a persistent kernel: every CTA slot of the device, at most ntiles
+// A launch that may begin while its stream predecessor finishes
+// (programmatic dependent launch; the kernel waits with griddepcontrol
+// before it touches memory).
+template <class... P, class... A>
+cudaError_t launch_chained(void (*kernel)(P...), int grid, int block, size_t smem, cudaStream_t s,
+                           A... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 template <class K>
 int persistent_grid(K kernel, size_t smem, long long ntiles, int *grid, int threads = NTHREADS) {
   int dev = 0, nsm = 0, per_sm = 0;
@@ -43,8 +62,8 @@ int launch_map_t(const Desc *d_descs, const int2 *d_tmap, long long ntiles, unsi
   }
   int grid = 0;
   persistent_grid(k_batch_map<FMA>, smem, ntiles, &grid);
-  k_batch_map<FMA><<<grid, NTHREADS, smem, s>>>(d_descs, d_tmap, ntiles, d_counter, d_status);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = launch_chained(k_batch_map<FMA>, grid, NTHREADS, smem, s, d_descs, d_tmap, ntiles,
+                                 d_counter, d_status);
   return e == cudaSuccess ? CGX_OK : cuda_error(e, "k_batch_map launch");
 }
 
@@ -92,9 +111,8 @@ int launch_tma_v(int variant, const Desc *d_descs, const CUtensorMap *d_maps, co
       per_sm < 1)
     per_sm = 1;
   const int grid = (int)std::min<long long>((long long)nsm * per_sm, ntiles);
-  k_tma_map<FMA, F, NTL, TK, CFG><<<grid, NT, smem, s>>>(d_descs, d_maps, d_tmap, ntiles, d_counter, d_status,
-                                                        variant);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = launch_chained(k_tma_map<FMA, F, NTL, TK, CFG>, grid, NT, smem, s, d_descs, d_maps, d_tmap,
+                                 ntiles, d_counter, d_status, variant);
   return e == cudaSuccess ? CGX_OK : cuda_error(e, "k_tma_map launch");
 }
 
@@ -119,8 +137,8 @@ int launch_stream_v(const Desc *d_descs, const int2 *d_tmap, long long ntiles,
                     unsigned long long *d_counter, int *d_status, cudaStream_t s) {
   int grid = 0;
   persistent_grid(k_stream_map<FMA, V>, 0, ntiles, &grid, STREAM_THREADS);
-  k_stream_map<FMA, V><<<grid, STREAM_THREADS, 0, s>>>(d_descs, d_tmap, ntiles, d_counter, d_status);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = launch_chained(k_stream_map<FMA, V>, grid, STREAM_THREADS, 0, s, d_descs, d_tmap, ntiles,
+                                 d_counter, d_status);
   return e == cudaSuccess ? CGX_OK : cuda_error(e, "k_stream_map launch");
 }
 

@@ -175,6 +175,28 @@ __global__ void __launch_bounds__(NTHREADS, 2)
   }
 }
 
+// ---------------------------------------------------------------- chaining
+// The persistent kernels of a batch run back to back with programmatic
+// dependent launch: a kernel waits for its predecessor's completion (and
+// memory) before it touches anything, and a CTA that has claimed its last
+// tile lets the successor's CTAs be scheduled.  Both are no-ops for a launch
+// without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Claim counters reset themselves, so that no memset precedes a launch:
+// counter[NSEG] counts the CTAs that have finished claiming, and the last
+// one zeroes both for the segment's next launch.  Called by thread 0 after
+// its last claim; the fence orders every CTA's claims before its count.
+__device__ __forceinline__ void claims_done(unsigned long long *counter) {
+  __threadfence();
+  unsigned long long *left = counter + NSEG;
+  if (atomicAdd(left, 1ULL) == (unsigned long long)gridDim.x - 1) {
+    atomicExch(counter, 0ULL);
+    atomicExch(left, 0ULL);
+  }
+}
+
 // Persistent form fed by a tile map: tmap[t] = (descriptor, tile within it).
 // Thread 0 claims the next tile when the current one starts, so the
 // claim's round trip overlaps the tile's work; only the map read is exposed.
@@ -186,6 +208,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
   __shared__ long long s_t;
   __shared__ int2 s_m;
   __shared__ __align__(16) Desc s_d;
+  pdl_wait();
   if (threadIdx.x == 0) {
     const long long t = (long long)atomicAdd(counter, 1ULL);
     s_t = t;
@@ -195,7 +218,10 @@ __global__ void __launch_bounds__(NTHREADS, 2)
   for (;;) {
     const long long t = s_t;
     const int2 m = s_m;
-    if (t >= ntiles) break;
+    if (t >= ntiles) {
+      if (threadIdx.x == 0) claims_done(counter);
+      break;
+    }
     if (threadIdx.x < sizeof(Desc) / 8)
       reinterpret_cast<unsigned long long *>(&s_d)[threadIdx.x] =
           __ldg(reinterpret_cast<const unsigned long long *>(descs + m.x) + threadIdx.x);
@@ -284,6 +310,7 @@ __global__ void __launch_bounds__(STREAM_THREADS, STREAM_MAP_BLOCKS_PER_SM)
       reinterpret_cast<unsigned long long *>(&s_d[buf])[tid] =
           __ldg(reinterpret_cast<const unsigned long long *>(descs + s_m[slot].x) + tid);
   };
+  pdl_wait();
   if (tid == 0) {
     claim(0);
     claim(1);
@@ -293,7 +320,11 @@ __global__ void __launch_bounds__(STREAM_THREADS, STREAM_MAP_BLOCKS_PER_SM)
   __syncthreads();
   for (int i = 0;; ++i) {
     const int slot = i % 3, buf = i & 1;
-    if (s_t[slot] >= ntiles) break;
+    if (s_t[slot] >= ntiles) {
+      if (tid == 0) claims_done(counter);
+      break;
+    }
+    if (s_t[(i + 1) % 3] >= ntiles) pdl_trigger(); // this CTA's last tile
     const int tile = s_m[slot].y;
     if (tid == 0) claim((i + 2) % 3);
     stage(buf ^ 1, (i + 1) % 3);
@@ -323,6 +354,7 @@ __global__ void __launch_bounds__(TMA_CFGS[CFG].nt, TMA_CFGS[CFG].mb)
   __shared__ __align__(16) Desc s_d;
   __shared__ __align__(8) uint64_t s_bars[TMA_NB_MAX];
   __shared__ int s_abort;
+  pdl_wait();
   if (threadIdx.x == 0) {
     for (int i = 0; i < TMA_NB_MAX; ++i) mbar_init(&s_bars[i], 1);
     mbar_fence_init();
@@ -334,15 +366,22 @@ __global__ void __launch_bounds__(TMA_CFGS[CFG].nt, TMA_CFGS[CFG].mb)
   __syncthreads();
   TmaRing ring{s_bars, &s_abort, 0u};
   for (;;) {
-    if (s_t >= ntiles) break;
+    if (s_t >= ntiles) {
+      if (threadIdx.x == 0) claims_done(counter);
+      break;
+    }
     const int2 m = s_m;
     if (threadIdx.x < sizeof(Desc) / 8)
       reinterpret_cast<unsigned long long *>(&s_d)[threadIdx.x] =
           __ldg(reinterpret_cast<const unsigned long long *>(descs + m.x) + threadIdx.x);
     if (threadIdx.x == 0) s_next = (long long)atomicAdd(counter, 1ULL);
     __syncthreads();
+    if (s_next >= ntiles) pdl_trigger(); // this CTA's last tile
     if (tma_variant(s_d) == variant) {
-      if (!prolong_tile_tma<F, FMA, NTL, TK, CFG>(s_d, maps + 3 * (size_t)m.x, m.y, sm, ring, status)) return;
+      if (!prolong_tile_tma<F, FMA, NTL, TK, CFG>(s_d, maps + 3 * (size_t)m.x, m.y, sm, ring, status)) {
+        if (threadIdx.x == 0) claims_done(counter);
+        return;
+      }
     } else if (threadIdx.x == 0) {
       report(status, CGX_EDEVICE);
     }

@@ -102,7 +102,9 @@ int slot_init(Slot &s, size_t desc_cap, size_t tile_cap) {
   if (e == cudaSuccess) e = cudaMallocHost(&s.h_maps, 3 * desc_cap * sizeof(CUtensorMap));
   if (e == cudaSuccess) e = cudaMalloc(&s.d_tmap, tile_cap * sizeof(int2));
   if (e == cudaSuccess) e = cudaMallocHost(&s.h_tmap, tile_cap * sizeof(int2));
-  if (e == cudaSuccess) e = cudaMalloc(&s.d_counter, NSEG * sizeof(unsigned long long));
+  // claim counters and exit counts (cgx_kernels.cuh, claims_done)
+  if (e == cudaSuccess) e = cudaMalloc(&s.d_counter, 2 * NSEG * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(s.d_counter, 0, 2 * NSEG * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMalloc(&s.d_status, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(s.d_status, 0, sizeof(int));
   if (e != cudaSuccess) return cuda_error(e, "server slot allocation");
