@@ -56,6 +56,11 @@ PHASE_KERNELS = {
 }
 
 
+# grid-function groups of the bench step (independent phase chains on
+# separate streams, see carpet_b200.amr.BergerOliger)
+GF_GROUPS = 2
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -76,6 +81,8 @@ def parse():
     p.add_argument("--tile-config", type=int, default=None,
                    help="pin every prolongation variant to this tile configuration instead of tuning")
     p.add_argument("--no-uneven", action="store_true", help="skip the batched uneven section")
+    p.add_argument("--gf-groups", type=int, default=GF_GROUPS,
+                   help="grid-function groups whose phase chains run on separate streams")
     p.add_argument("--moving", action="store_true",
                    help="add the moving-box section (~80 GB on the device, minutes)")
     return p.parse_args()
@@ -524,17 +531,16 @@ def main():
     h = nested(args.levels, args.npoints, ghost=3, buffer=9, order=5)
     st = Storage(h, args.ngf, 3)
     fill_storage(st, h, seed=1 + rank)
-    bo = BergerOliger(h, st, order_space=5, order_time=2)
+    bo = BergerOliger(h, st, order_space=5, order_time=2, groups=args.gf_groups)
     steps3 = [bo.step_phases() for _ in range(3)]  # the rotation repeats every 3 steps
     for keys in steps3:
         for k in keys:
-            bo.batch(k)
+            bo.group_batches(k)
     tuned, tuned_by_key = {}, {}
     if args.tile_config is not None:
         for keys in steps3:
+            bo.set_config(keys, args.tile_config)
             for k in keys:
-                bo.batch(k).set_config(args.tile_config)
-                bo.batch(k).upload()
                 tuned_by_key[k] = {v: args.tile_config for v in range(40)}
         tuned = {"all": {0: args.tile_config}}
     elif not args.no_tune:
@@ -584,20 +590,21 @@ def main():
     # is a homogeneous batch, i.e. one kernel; the dominant kernel is the
     # phase kind with the largest share of the step
     keys = steps3[(args.warmup + args.steps) % 3]
+    launches = [(k, b) for k in keys for b in bo.group_batches(k)]
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in keys]
-    for (a, b_), k in zip(evs, keys):
+           for _ in launches]
+    for (a, b_), (k, b) in zip(evs, launches):
         a.record(stream)
-        bo.batch(k).launch(stream)
+        b.launch(stream)
         b_.record(stream)
     stream.synchronize()
     phases = {}
-    for (a, b_), k in zip(evs, keys):
+    for (a, b_), (k, b) in zip(evs, launches):
         name = PHASE_KERNELS[(k[0], k[3])]
         e = phases.setdefault(name, {"launches": 0, "ms": 0.0, "bytes": 0})
         e["launches"] += 1
         e["ms"] += a.elapsed_time(b_)
-        e["bytes"] += bo.batch(k).stats()["bytes"]
+        e["bytes"] += b.stats()["bytes"]
     tot_ms = sum(e["ms"] for e in phases.values())
     for e in phases.values():
         e["gbs"] = round(e["bytes"] / (e["ms"] * 1e-3) / 1e9, 1)
@@ -649,13 +656,14 @@ def main():
         for la, lb in zip(st.pools, stB.pools):
             for p, q in zip(la, lb):
                 q.copy_(p)
-        boB = BergerOliger(h, stB, order_space=5, order_time=2)
+        boB = BergerOliger(h, stB, order_space=5, order_time=2, groups=args.gf_groups)
         stepsB = [boB.step_phases() for _ in range(3)]
         for keys in stepsB:
             for k in keys:
-                for v, c in tuned_by_key.get(k, {}).items():
-                    boB.batch(k).set_config(c, v)
-                boB.batch(k).upload()
+                for b in boB.group_batches(k):
+                    for v, c in tuned_by_key.get(k, {}).items():
+                        b.set_config(c, v)
+                    b.upload()
         graphsB = []
         for keys in stepsB:
             g = cb.Graph()
@@ -746,6 +754,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "fp_mode": args.fp, "ngf": args.ngf,
+                       "gf_groups": args.gf_groups,
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (~10 GB per step)",
                        "bytes_per_step": int(bytes_step), "fine_points_per_step": int(points_step),

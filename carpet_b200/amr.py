@@ -20,6 +20,11 @@ side) is not part of the transfer path and is not run.
 
 Each such phase is one batch of box-pairs over all grid functions, run by
 the persistent kernel; a whole coarse step can be captured as a CUDA graph.
+Grid functions never exchange data, so with ``groups`` > 1 the grid
+functions are split into that many groups whose phase chains run on
+separate streams: each group keeps the reference's call order, and one
+group's kernels fill the SMs that another group's kernel leaves idle while
+its last tiles drain.
 """
 from __future__ import annotations
 
@@ -128,8 +133,12 @@ class BergerOliger:
     """Transfer phases of one coarse step of a nested hierarchy."""
 
     def __init__(self, h: Hierarchy, st: Storage, order_space=5, order_time=2,
-                 op=OP_LAGRANGE, cent=VERTEX):
+                 op=OP_LAGRANGE, cent=VERTEX, groups: int = 1):
+        if not 1 <= groups <= st.ngf:
+            raise ValueError("groups must lie in 1..ngf")
         self.h, self.st = h, st
+        self.groups = groups
+        self._side: List[torch.cuda.Stream] = []
         self.order_space, self.order_time = order_space, order_time
         self.op, self.cent = op, cent
         self.L = len(h.levels)
@@ -143,15 +152,22 @@ class BergerOliger:
     def _tl(self, l, r, tl):
         return self.st.data[l][self.pool_index(r, tl)]
 
-    def _build(self, key) -> Batch:
+    def gfs(self, grp: int) -> range:
+        """grid functions of group grp (contiguous, sizes differing by one
+        at most)"""
+        n, G = self.st.ngf, self.groups
+        return range(grp * n // G, (grp + 1) * n // G)
+
+    def _build(self, key, grp: int) -> Batch:
         kind, l, rots, ntl = key
         b = Batch()
         h, st = self.h, self.st
+        gfs = self.gfs(grp)
         if kind == "sync":
             r, = rots
             arrs = self._tl(l, r, 0)
             b.add_many([(arrs[g][p.dst_comp], [arrs[g][p.src_comp]], p.dstbox, p.srcbox)
-                        for g in range(st.ngf) for p in h.sync[l]],
+                        for g in gfs for p in h.sync[l]],
                        [0.0], 0.0, 1, 0, op=self.op, cent=self.cent)
         elif kind == "prolong":
             rf, rc = rots
@@ -163,22 +179,27 @@ class BergerOliger:
             times = [0.0, -dtc, -2 * dtc]
             time = -dtc / 2 if ntl > 1 else 0.0
             b.add_many([(dst[g][p.dst_comp], [s[g][p.src_comp] for s in srcs], p.dstbox, p.srcbox)
-                        for g in range(st.ngf) for p in h.prolong[l]],
+                        for g in gfs for p in h.prolong[l]],
                        times, time, self.order_space, self.order_time, op=self.op, cent=self.cent)
         elif kind == "restrict":
             rc, rf = rots
             dst = self._tl(l, rc, 0)
             src = self._tl(l + 1, rf, 0)
             b.add_many([(dst[g][p.dst_comp], [src[g][p.src_comp]], p.dstbox, p.srcbox)
-                        for g in range(st.ngf) for p in h.restrict[l + 1]],
+                        for g in gfs for p in h.restrict[l + 1]],
                        [0.0], 0.0, self.order_space, 0, op=self.op, cent=self.cent)
         b.upload()
         return b
 
-    def batch(self, key) -> Batch:
-        if key not in self.batches:
-            self.batches[key] = self._build(key)
-        return self.batches[key]
+    def batch(self, key, grp: int = 0) -> Batch:
+        """the batch of phase key for grid-function group grp"""
+        k = key if grp == 0 else key + (grp,)
+        if k not in self.batches:
+            self.batches[k] = self._build(key, grp)
+        return self.batches[k]
+
+    def group_batches(self, key) -> List[Batch]:
+        return [self.batch(key, g) for g in range(self.groups)]
 
     def step_phases(self) -> List[tuple]:
         """the phases of one coarse step, advancing the rotation state"""
@@ -204,26 +225,62 @@ class BergerOliger:
 
     def autotune(self, keys, reps=2, stream=None):
         """tile configurations of every phase's prolongation kernels, chosen
-        by timing (runs the phases); returns {phase: {variant: config}}"""
-        return {k: self.batch(k).autotune(reps, stream) for k in dict.fromkeys(keys)}
+        by timing group 0's batch (runs the phases; the groups have the same
+        box-pairs); returns {phase: {variant: config}}"""
+        out = {}
+        for k in dict.fromkeys(keys):
+            out[k] = cfg = self.batch(k).autotune(reps, stream)
+            for b in self.group_batches(k)[1:]:
+                for v, c in cfg.items():
+                    b.set_config(c, v)
+                b.upload(stream)
+        return out
+
+    def set_config(self, keys, config: int, stream=None):
+        """pin every prolongation variant of the phases' batches to one tile
+        configuration"""
+        for k in dict.fromkeys(keys):
+            for b in self.group_batches(k):
+                b.set_config(config)
+                b.upload(stream)
 
     def run(self, keys, stream=None, per_box=False):
-        for k in keys:
-            b = self.batch(k)
-            if per_box:
-                b.launch_per_box(stream)
-            else:
-                b.launch(stream)
+        """launch the phases in order; with several groups, group g's chain
+        runs on its own stream, forked from and joined back into stream
+        (which may be capturing a graph)"""
+        if self.groups == 1:
+            for k in keys:
+                b = self.batch(k)
+                if per_box:
+                    b.launch_per_box(stream)
+                else:
+                    b.launch(stream)
+            return
+        main = stream if stream is not None else torch.cuda.current_stream()
+        while len(self._side) < self.groups - 1:
+            self._side.append(torch.cuda.Stream(device=main.device))
+        streams = [main] + self._side[:self.groups - 1]
+        for s in streams[1:]:
+            s.wait_stream(main)
+        for g, s in enumerate(streams):
+            for k in keys:
+                b = self.batch(k, g)
+                if per_box:
+                    b.launch_per_box(s)
+                else:
+                    b.launch(s)
+        for s in streams[1:]:
+            main.wait_stream(s)
 
     def stats(self, keys):
         """totals over the phases: box-pairs, tiles, points, algorithmic
         bytes, batches (phases) and kernel launches"""
         tot = dict(pairs=0, tiles=0, points=0, bytes=0, launches=0, kernels=0)
         for k in keys:
-            b = self.batch(k)
-            s = b.stats()
-            for n in ("pairs", "tiles", "points", "bytes"):
-                tot[n] += s[n]
-            tot["launches"] += 1
-            tot["kernels"] += b.kernels()
+            for b in self.group_batches(k):
+                s = b.stats()
+                for n in ("pairs", "tiles", "points", "bytes"):
+                    tot[n] += s[n]
+                tot["launches"] += 1
+                tot["kernels"] += b.kernels()
         return tot

@@ -13,7 +13,10 @@ injection and ghost sync -- one coarse Berger-Oliger step, FMA mode.
   leave every point of every array bit-identical;
 * the batched kernels (TMA-staged prolongation, persistent streaming
   kernels) and the per-box kernels (cp.async-staged prolongation, per-box
-  streaming) give the same bits on the whole step.
+  streaming) give the same bits on the whole step;
+* the grid functions split into groups whose phase chains run on separate
+  streams (eagerly and captured as one graph) give the same bits as one
+  chain over all of them.
 """
 import numpy as np
 import pytest
@@ -35,14 +38,14 @@ def cgx():
     return cb
 
 
-def workload(cb, ngf, fill):
+def workload(cb, ngf, fill, groups=1):
     from carpet_b200.amr import BergerOliger, Storage
     from carpet_b200.hierarchy import nested
     cb.set_fp_mode(True)
     h = nested(LEVELS, NPOINTS, ghost=3, buffer=9, order=5)
     st = Storage(h, ngf, 3)
     fill(st, h)
-    bo = BergerOliger(h, st, order_space=5, order_time=2)
+    bo = BergerOliger(h, st, order_space=5, order_time=2, groups=groups)
     return h, st, bo
 
 
@@ -165,3 +168,37 @@ def test_batched_and_per_box_kernels_agree_on_the_step(cgx):
     for l, (lp, bp) in enumerate(zip(st.pools, batched)):
         for p, q in zip(lp, bp):
             assert torch.equal(p.view(torch.int64), q.view(torch.int64)), ("level", l)
+
+
+@pytest.mark.parametrize("groups", [2, 3])
+def test_grid_function_groups_on_streams_match_one_chain(cgx, groups):
+    ngf = 5
+    _, st1, bo1 = workload(cgx, ngf, random_fill)
+    _, st2, bo2 = workload(cgx, ngf, random_fill, groups=groups)
+    parts = [list(bo2.gfs(g)) for g in range(groups)]
+    assert sum(parts, []) == list(range(ngf)) and all(parts)
+    stream = torch.cuda.Stream()
+    # step 1 eagerly, step 2 from a captured graph (the fork and join of the
+    # groups' streams inside the capture)
+    keys1 = bo1.step_phases()
+    keys2 = bo2.step_phases()
+    assert keys1 == keys2
+    bo1.run(keys1, stream)
+    bo2.run(keys2, stream)
+    keys1 = bo1.step_phases()
+    keys2 = bo2.step_phases()
+    for k in keys2:  # build and upload outside the capture
+        bo2.group_batches(k)
+    stream.synchronize()
+    g = cgx.Graph()
+    with g.capture(stream):
+        bo2.run(keys2, stream)
+    bo1.run(keys1, stream)
+    g.launch(stream)
+    for b in list(bo1.batches.values()) + list(bo2.batches.values()):
+        b.check(stream)
+    stream.synchronize()
+    for l, (p1, p2) in enumerate(zip(st1.pools, st2.pools)):
+        for a, b in zip(p1, p2):
+            assert torch.equal(a.view(torch.int64), b.view(torch.int64)), ("level", l)
+    del g
