@@ -59,6 +59,8 @@ PHASE_KERNELS = {
 # grid-function groups of the bench step (independent phase chains on
 # separate streams, see carpet_b200.amr.BergerOliger)
 GF_GROUPS = 2
+# phases by which each further group starts after the first
+GF_STAGGER = 0
 
 
 def parse():
@@ -83,6 +85,8 @@ def parse():
     p.add_argument("--no-uneven", action="store_true", help="skip the batched uneven section")
     p.add_argument("--gf-groups", type=int, default=GF_GROUPS,
                    help="grid-function groups whose phase chains run on separate streams")
+    p.add_argument("--gf-stagger", type=int, default=GF_STAGGER,
+                   help="phases by which each further grid-function group starts after the first")
     p.add_argument("--moving", action="store_true",
                    help="add the moving-box section (~80 GB on the device, minutes)")
     return p.parse_args()
@@ -531,7 +535,8 @@ def main():
     h = nested(args.levels, args.npoints, ghost=3, buffer=9, order=5)
     st = Storage(h, args.ngf, 3)
     fill_storage(st, h, seed=1 + rank)
-    bo = BergerOliger(h, st, order_space=5, order_time=2, groups=args.gf_groups)
+    bo = BergerOliger(h, st, order_space=5, order_time=2, groups=args.gf_groups,
+                      stagger=args.gf_stagger)
     steps3 = [bo.step_phases() for _ in range(3)]  # the rotation repeats every 3 steps
     for keys in steps3:
         for k in keys:
@@ -671,7 +676,8 @@ def main():
         for la, lb in zip(st.pools, stB.pools):
             for p, q in zip(la, lb):
                 q.copy_(p)
-        boB = BergerOliger(h, stB, order_space=5, order_time=2, groups=args.gf_groups)
+        boB = BergerOliger(h, stB, order_space=5, order_time=2, groups=args.gf_groups,
+                           stagger=args.gf_stagger)
         stepsB = [boB.step_phases() for _ in range(3)]
         for keys in stepsB:
             for k in keys:
@@ -769,7 +775,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "fp_mode": args.fp, "ngf": args.ngf,
-                       "gf_groups": args.gf_groups,
+                       "gf_groups": args.gf_groups, "gf_stagger": args.gf_stagger,
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (~10 GB per step)",
                        "bytes_per_step": int(bytes_step), "fine_points_per_step": int(points_step),

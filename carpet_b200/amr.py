@@ -133,11 +133,13 @@ class BergerOliger:
     """Transfer phases of one coarse step of a nested hierarchy."""
 
     def __init__(self, h: Hierarchy, st: Storage, order_space=5, order_time=2,
-                 op=OP_LAGRANGE, cent=VERTEX, groups: int = 1):
+                 op=OP_LAGRANGE, cent=VERTEX, groups: int = 1, stagger: int = 0):
         if not 1 <= groups <= st.ngf:
             raise ValueError("groups must lie in 1..ngf")
+        if stagger < 0:
+            raise ValueError("stagger must not be negative")
         self.h, self.st = h, st
-        self.groups = groups
+        self.groups, self.stagger = groups, stagger
         self._side: List[torch.cuda.Stream] = []
         self.order_space, self.order_time = order_space, order_time
         self.op, self.cent = op, cent
@@ -244,32 +246,43 @@ class BergerOliger:
                 b.set_config(config)
                 b.upload(stream)
 
-    def run(self, keys, stream=None, per_box=False):
+    def run(self, keys, stream=None, per_box=False, stagger=None):
         """launch the phases in order; with several groups, group g's chain
         runs on its own stream, forked from and joined back into stream
-        (which may be capturing a graph)"""
+        (which may be capturing a graph).  With stagger > 0 group g starts
+        once group 0 has completed g * stagger phases, so that the groups'
+        concurrent kernels are of different kinds."""
+        if stagger is None:
+            stagger = self.stagger
+
+        def launch(b, s):
+            if per_box:
+                b.launch_per_box(s)
+            else:
+                b.launch(s)
         if self.groups == 1:
             for k in keys:
-                b = self.batch(k)
-                if per_box:
-                    b.launch_per_box(stream)
-                else:
-                    b.launch(stream)
+                launch(self.batch(k), stream)
             return
         main = stream if stream is not None else torch.cuda.current_stream()
         while len(self._side) < self.groups - 1:
             self._side.append(torch.cuda.Stream(device=main.device))
-        streams = [main] + self._side[:self.groups - 1]
-        for s in streams[1:]:
-            s.wait_stream(main)
-        for g, s in enumerate(streams):
-            for k in keys:
-                b = self.batch(k, g)
-                if per_box:
-                    b.launch_per_box(s)
-                else:
-                    b.launch(s)
-        for s in streams[1:]:
+        side = self._side[:self.groups - 1]
+        fork_at = {min(g * stagger, len(keys)): [] for g in range(1, self.groups)}
+        for g in range(1, self.groups):
+            fork_at[min(g * stagger, len(keys))].append(g)
+
+        def fork(gs):
+            for g in gs:
+                s = side[g - 1]
+                s.wait_stream(main)
+                for k in keys:
+                    launch(self.batch(k, g), s)
+        for j, k in enumerate(keys):
+            fork(fork_at.get(j, []))
+            launch(self.batch(k, 0), main)
+        fork(fork_at.get(len(keys), []))
+        for s in side:
             main.wait_stream(s)
 
     def stats(self, keys):

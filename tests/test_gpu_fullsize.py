@@ -15,8 +15,9 @@ injection and ghost sync -- one coarse Berger-Oliger step, FMA mode.
   kernels) and the per-box kernels (cp.async-staged prolongation, per-box
   streaming) give the same bits on the whole step;
 * the grid functions split into groups whose phase chains run on separate
-  streams (eagerly and captured as one graph) give the same bits as one
-  chain over all of them.
+  streams (eagerly and captured as one graph, the groups started together
+  or staggered by whole phases) give the same bits as one chain over all
+  of them.
 """
 import numpy as np
 import pytest
@@ -170,11 +171,12 @@ def test_batched_and_per_box_kernels_agree_on_the_step(cgx):
             assert torch.equal(p.view(torch.int64), q.view(torch.int64)), ("level", l)
 
 
-@pytest.mark.parametrize("groups", [2, 3])
-def test_grid_function_groups_on_streams_match_one_chain(cgx, groups):
+@pytest.mark.parametrize("groups,stagger", [(2, 0), (3, 0), (2, 1), (3, 2)])
+def test_grid_function_groups_on_streams_match_one_chain(cgx, groups, stagger):
     ngf = 5
     _, st1, bo1 = workload(cgx, ngf, random_fill)
     _, st2, bo2 = workload(cgx, ngf, random_fill, groups=groups)
+    bo2.stagger = stagger
     parts = [list(bo2.gfs(g)) for g in range(groups)]
     assert sum(parts, []) == list(range(ngf)) and all(parts)
     stream = torch.cuda.Stream()
