@@ -437,8 +437,8 @@ def moving(ngf: int, fp: str, steps: int):
     st = Storage(h0, ngf, 3)
     fill_storage(st, h0, seed=5)
     s = torch.cuda.Stream()
-    # one coarse step
-    bo = BergerOliger(h0, st, order_space=5, order_time=2)
+    # one coarse step (grid-function groups on streams, as the main step)
+    bo = BergerOliger(h0, st, order_space=5, order_time=2, groups=min(GF_GROUPS, ngf))
     keys = bo.step_phases()
     tuned = bo.autotune(keys, reps=3)
     g = cb.Graph()
@@ -483,7 +483,7 @@ def moving(ngf: int, fp: str, steps: int):
                        "regrid after 8 coarse steps",
            "resident_gb": round(st.nbytes() / 1e9, 1),
            "step_ms": round(step_ms, 2), "step_gbs": round(sst["bytes"] / (step_ms * 1e-3) / 1e9, 1),
-           "step_phases": len(keys), "step_kernels": sst["kernels"],
+           "step_phases": len(keys), "step_kernels": sst["kernels"], "gf_groups": bo.groups,
            "regrid_host_ms": round((tb - t0 + t2 - t1) * 1e3, 1),
            "regrid_alloc_ms": round((t1 - tb) * 1e3, 1),
            "regrid_fill_ms": round(fill_ms, 3),
