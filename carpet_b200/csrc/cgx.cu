@@ -774,6 +774,10 @@ struct cgx_batch {
   double *d_tmp = nullptr;
   size_t tmp_cap = 0;    // doubles
   std::vector<Desc> pdescs; // descs with the temporaries bound
+  // streams and events of the concurrent segment launch (created on first
+  // use, on the device current then)
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> ev; // ev[0] forks, ev[1 + k] joins side[k]
 };
 
 namespace {
@@ -899,6 +903,8 @@ int cgx_batch_destroy(cgx_batch *b) {
   cudaFree(b->d_counter);
   cudaFree(b->d_status);
   cudaFree(b->d_tmp);
+  for (cudaStream_t x : b->side) cudaStreamDestroy(x);
+  for (cudaEvent_t x : b->ev) cudaEventDestroy(x);
   delete b;
   return CGX_OK;
 }
@@ -1059,6 +1065,67 @@ int cgx_batch_upload(cgx_batch *b, void *stream) {
   return CGX_OK;
 }
 
+// The tile map's segments, one kernel each.  Pairs of a batch write
+// disjoint points and read none that another pair writes, so the segments
+// are independent, except the time-combination segment (the last), which
+// reads the temporaries that its staged pairs' first stages write in the
+// other segments.  Every other non-empty segment therefore runs on a
+// stream of its own, forked from s and joined back into it (which also
+// works while s is being captured), and the time segment runs on s after
+// the join.  A batch with one such segment launches as one chain on s.
+static int launch_segments(cgx_batch *b, cudaStream_t s) {
+  constexpr int TSEG = SEG_STREAM + SV_TIME;
+  static_assert(TSEG == NSEG - 1, "the time combination is the last segment");
+  int idx[NSEG], n = 0;
+  for (int i = 0; i < TSEG; ++i)
+    if (b->seg[i + 1] > b->seg[i]) idx[n++] = i;
+  if (n <= 1)
+    return launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, b->seg, b->tma_cfg, b->d_counter,
+                      b->d_status, s);
+  const size_t nside = (size_t)n - 1;
+  cudaError_t e = cudaSuccess;
+  while (b->side.size() < nside) {
+    cudaStream_t x = nullptr;
+    e = cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreateWithFlags");
+    b->side.push_back(x);
+  }
+  while (b->ev.size() < nside + 1) {
+    cudaEvent_t x = nullptr;
+    e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaEventCreateWithFlags");
+    b->ev.push_back(x);
+  }
+  // a segment array in which only segment i is non-empty
+  auto only = [&](int i, long long *sg) {
+    for (int k = 0; k <= NSEG; ++k) sg[k] = k <= i ? b->seg[i] : b->seg[i + 1];
+  };
+  e = cudaEventRecord(b->ev[0], s);
+  for (size_t k = 0; k < nside && e == cudaSuccess; ++k) e = cudaStreamWaitEvent(b->side[k], b->ev[0], 0);
+  if (e != cudaSuccess) return cuda_fail(e, "fork of the segment streams");
+  int rc = CGX_OK;
+  for (int j = 0; j < n && rc == CGX_OK; ++j) {
+    long long sg[NSEG + 1];
+    only(idx[j], sg);
+    rc = launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, sg, b->tma_cfg, b->d_counter, b->d_status,
+                    j == 0 ? s : b->side[j - 1]);
+  }
+  // join every side stream, also after a failed launch
+  for (size_t k = 0; k < nside; ++k) {
+    cudaError_t r = cudaEventRecord(b->ev[1 + k], b->side[k]);
+    if (r == cudaSuccess) r = cudaStreamWaitEvent(s, b->ev[1 + k], 0);
+    if (r != cudaSuccess && e == cudaSuccess) e = r;
+  }
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_fail(e, "join of the segment streams");
+  if (b->seg[TSEG + 1] > b->seg[TSEG]) {
+    long long sg[NSEG + 1];
+    only(TSEG, sg);
+    rc = launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, sg, b->tma_cfg, b->d_counter, b->d_status, s);
+  }
+  return rc;
+}
+
 int cgx_batch_launch(cgx_batch *b, void *stream) {
   if (!b) return fail(CGX_EINVAL, "null batch");
   cudaStream_t s = (cudaStream_t)stream;
@@ -1070,9 +1137,8 @@ int cgx_batch_launch(cgx_batch *b, void *stream) {
   }
   if (b->n_uploaded > 0) {
     // the segment kernels leave their counters at zero: no memset between
-    // the launches, which run chained
-    int rc = launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, b->seg, b->tma_cfg, b->d_counter,
-                        b->d_status, s);
+    // the launches, which run chained on each stream
+    int rc = launch_segments(b, s);
     if (rc) return rc;
   }
   return CGX_OK;
