@@ -155,7 +155,10 @@ int cgx_batch_stats(const cgx_batch *b, int64_t *npairs, int64_t *ntiles,
 int cgx_batch_upload(cgx_batch *b, void *stream);
 /* the uploaded box-pairs, one persistent kernel per kind of tile (a
  * homogeneous batch -- one operator, order and timelevel count -- is one
- * kernel) */
+ * kernel).  Several kernels run concurrently on streams the batch owns,
+ * forked from and joined back into `stream` (also inside a capture); the
+ * time combination of staged transfers runs last, on `stream`.  Work issued
+ * on `stream` after the call waits for all of it. */
 int cgx_batch_launch(cgx_batch *b, void *stream);
 /* kernels one cgx_batch_launch issues for the current upload (no
  * counterpart in the reference: a measurement aid) */
