@@ -72,8 +72,13 @@ def parse():
     p.add_argument("--ngf", type=int, default=25)
     p.add_argument("--npoints", type=int, default=129)
     p.add_argument("--levels", type=int, default=5)
-    p.add_argument("--fp", default="fma", choices=["exact", "fma"])
-    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--fp", default="exact", choices=["exact", "fma"],
+                   help="exact: the reference's operation order with two roundings per "
+                        "multiply-add (bit-exact); fma: fused multiply-adds")
+    p.add_argument("--cpu-seconds", type=float, default=15.0,
+                   help="host time of the CPU baseline leg of the GPU arm")
+    p.add_argument("--ref-seconds", type=float, default=2.0,
+                   help="host time per step of the reference arm (sets the grid functions per step)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
@@ -221,103 +226,62 @@ def fill_storage(st, h, seed=1):
 
 
 # ----------------------------------------------------------------- CPU arm
-def coarse_points(reg, srcbbox, order=5):
-    """coarse points an order-5 vertex-centred prolongation of ``reg`` reads
-    (the algorithmic source bytes the library counts per timelevel)"""
-    lo1, hi1 = -(order // 2), order // 2 + 1
-    n = 1
-    for d in range(3):
-        soff = (reg[d] - srcbbox[d]) // reg[6 + d]
-        m = (reg[3 + d] - reg[d]) // reg[6 + d] + 1
-        cs = [(soff + i) for i in range(min(2, m))] + [(soff + i) for i in range(max(0, m - 2), m)]
-        lo = min((s >> 1) + (lo1 if s & 1 else 0) for s in cs)
-        hi = max((s >> 1) + (hi1 if s & 1 else 0) for s in cs)
-        n *= hi - lo + 1
-    return n
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
 
 
-def cpu_sample(h, ngf, seconds, prefer_ref=True):
-    """CarpetLib's operators on the host: the transfers of the finest level's
-    first two substeps (boundary prolongation with and without time
-    interpolation, sync) and one restriction, for as many grid functions as
-    fit the time budget.  Returns (GB/s, cores, kind, sample description)."""
-    import numpy as np
-    from oracle.binding import Port, Ref, alloc
-    from carpet_b200.hierarchy import npoints, size
-    if prefer_ref and Ref.available():
-        lib, kind = Ref(False), "reference"
-        lib.set_openmp(True)
-        cores = os.cpu_count()
-    else:
-        lib, kind = Port(), "port"
-        cores = 1
+def cpu_reference(h, ngf, seconds_per_step, steps, warmup):
+    """CarpetLib's own operators on the host cores (oracle/_ref, compiled
+    from the reference sources; OpenMP over every core with the reference's
+    call_operator split): the WHOLE coarse Berger-Oliger step -- every phase
+    of every level in the call order of Carpet/src/Evolve.cc:44-121, through
+    data<T>::transfer_time with its per-call temporaries -- for as many grid
+    functions as fit ``seconds_per_step`` (grid functions are independent,
+    so the rate per grid function is the rate of the step).  Every build
+    present is calibrated on one grid function; the fastest is timed over
+    ``warmup`` + ``steps`` steps.  Returns a dict for the JSON line."""
+    from carpet_b200 import bo
+    from oracle.bo_step import RefStep, builds
+    found = builds()
+    if not found:
+        return None
     L = len(h.levels)
-    lf, lc = h.levels[L - 1], h.levels[L - 2]
-    rng = np.random.default_rng(7)
-
-    def arrays(lev):
-        return [alloc(c.exterior) for c in lev.comps]
-
-    def filled(lev):
-        out = arrays(lev)
-        for a in out:
-            a[...] = rng.standard_normal(a.shape)
-        return out
-
-    fine = filled(lf)
-    coarse = [filled(lc) for _ in range(3)]
-    dtc = 1.0 / 64
-    times = [0.0, -dtc, -2 * dtc]
-    tmp_cache = {}
-
-    def prolong(ntl):
-        by = 0
-        for p in h.prolong[L - 1]:
-            dst, db = fine[p.dst_comp], lf.comps[p.dst_comp].exterior
-            sb = lc.comps[p.src_comp].exterior
-            if ntl == 1:
-                lib.prolongate_3d_rf2(5, coarse[0][p.src_comp], sb, dst, db, p.dstbox)
-            else:
-                key = p.dstbox
-                if key not in tmp_cache:
-                    tmp_cache[key] = [alloc(p.dstbox, pad_x_even=False) for _ in range(3)]
-                tmps = tmp_cache[key]
-                for t in range(3):
-                    lib.prolongate_3d_rf2(5, coarse[t][p.src_comp], sb, tmps[t], p.dstbox, p.dstbox)
-                lib.interpolate_3d_3tl(tmps, times, p.dstbox, dst, db, p.dstbox, -dtc / 2)
-            by += 8 * npoints(p.dstbox) + ntl * 8 * coarse_points(p.dstbox, sb)
-        return by
-
-    def sync():
-        by = 0
-        for p in h.sync[L - 1]:
-            lib.copy_3d(fine[p.src_comp], lf.comps[p.src_comp].exterior, fine[p.dst_comp],
-                        lf.comps[p.dst_comp].exterior, p.srcbox, p.dstbox)
-            by += 16 * npoints(p.dstbox)
-        return by
-
-    def restrict():
-        by = 0
-        for p in h.restrict[L - 1]:
-            lib.restrict_3d_rf2(fine[p.src_comp], lf.comps[p.src_comp].exterior,
-                                coarse[0][p.dst_comp], lc.comps[p.dst_comp].exterior, p.dstbox)
-            by += 16 * npoints(p.dstbox)
-        return by
-
-    # one grid function's worth of the sample, repeated within the budget
-    t0 = time.perf_counter()
-    total, reps = 0, 0
-    while True:
-        total += prolong(3) + sync() + prolong(1) + sync() + restrict()
-        reps += 1
+    rates = {}
+    cal = {}
+    for name, path in found:
+        rs = RefStep(h, 1, path=path)
+        rot = [0] * L
+        rs.run(bo.step_phases(L, 3, rot))  # warm: page in, build the call lists
+        keys = bo.step_phases(L, 3, rot)
+        t0 = time.perf_counter()
+        nb = rs.run(keys)
         el = time.perf_counter() - t0
-        if el >= seconds or reps >= ngf:
-            break
-    el = time.perf_counter() - t0
-    sample = (f"finest level of the workload: 2 boundary prolongations (3-TL and 1-TL), "
-              f"2 syncs, 1 restriction; {reps} grid function(s); {total / 1e9:.2f} GB "
-              f"algorithmic in {el:.1f} s")
-    return total / el / 1e9, cores, kind, sample
+        rates[name] = round(nb / el / 1e9, 3)
+        cal[name] = (path, el)
+        del rs
+    best = max(rates, key=rates.get)
+    path, t1 = cal[best]
+    ng = max(1, min(ngf, int(seconds_per_step / t1)))
+    rs = RefStep(h, ng, path=path)
+    rot = [0] * L
+    for _ in range(max(1, warmup)):
+        rs.run(bo.step_phases(L, 3, rot))
+    total, el = 0, 0.0
+    for _ in range(steps):
+        keys = bo.step_phases(L, 3, rot)
+        t0 = time.perf_counter()
+        total += rs.run(keys)
+        el += time.perf_counter() - t0
+    v = total / el / 1e9
+    return {"value": round(v, 3), "unit": "GB/s", "cores": host_cores(), "kind": "reference",
+            "build": best, "builds_gbs": rates, "ms_per_step": round(el / steps * 1e3, 2),
+            "sample": f"the whole coarse step (91 phases, 5 levels) for {ng} of the {ngf} grid "
+                      f"functions per step, {steps} step(s) after {max(1, warmup)} warm-up; "
+                      f"{total / 1e9:.2f} GB algorithmic in {el:.1f} s; fastest of "
+                      f"{len(rates)} reference build(s)"}
 
 
 # ----------------------------------------------------------------- served
@@ -495,30 +459,43 @@ def moving(ngf: int, fp: str, steps: int):
 
 
 # ----------------------------------------------------------------- main
+def workload_config(args, bytes_step, points_step):
+    """the workload, identical in both arms' JSON lines"""
+    return {"workload": WORKLOAD, "levels": args.levels, "points_per_level": args.npoints,
+            "components_per_level": 8, "ngf": args.ngf, "ntl": 3,
+            "bytes_per_step": int(bytes_step), "fine_points_per_step": int(points_step),
+            "l2": "inputs larger than L2 (~16 GB algorithmic per step)"}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
 
     if args.impl == "reference":
+        # rank 0 alone; the other ranks exit without work.  Nothing here
+        # loads libcgx.so: the schedule is the pure-Python one.
         if rank != 0:
             return
         from carpet_b200.hierarchy import nested
-        h = nested(args.levels, args.npoints, ghost=3, buffer=9, order=5)
-        vals = []
-        for s in range(args.warmup + args.steps):
-            gbs, cores, kind, sample = cpu_sample(h, args.ngf, args.cpu_seconds / 3)
-            if s >= args.warmup:
-                vals.append(gbs)
-        v = sorted(vals)[len(vals) // 2]
+        h = nested(args.levels, args.npoints, ghost=3, buffer=9, order=5, native=False)
+        from carpet_b200.bo import workload_totals
+        bytes_step, points_step = workload_totals(h, args.ngf)
+        ref = cpu_reference(h, args.ngf, args.ref_seconds, args.steps, args.warmup)
+        if ref is None:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference operators are not "
+                              "built (oracle/_ref): run make -C oracle ref where the sources are"}))
+            return
+        v = ref["value"]
         print(json.dumps({
-            "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "GB/s",
+            "impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ref["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "parallelism": "host cores"},
-            "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": cores, "kind": kind,
-                             "sample": sample},
-            "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+            "data": "synthetic", "config": workload_config(args, bytes_step, points_step),
+            "parallelism": f"host cores (OpenMP, {ref['cores']} threads)",
+            "cpu_baseline": ref,
+            "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}))
         return
 
@@ -557,6 +534,11 @@ def main():
     stats = [bo.stats(k) for k in steps3]
     bytes_step = sum(s["bytes"] for s in stats) / 3
     points_step = sum(s["points"] for s in stats) / 3
+    # the library's count (from its descriptors) against the host count of
+    # the schedule that the reference arm prints
+    from carpet_b200.bo import workload_totals
+    if (int(bytes_step), int(points_step)) != tuple(int(x) for x in workload_totals(h, args.ngf)):
+        raise RuntimeError("algorithmic byte counts of the library and the schedule differ")
     kernels_step = sum(s["kernels"] for s in stats) / 3
     stream = torch.cuda.Stream()
     torch.cuda.synchronize()
@@ -742,9 +724,10 @@ def main():
 
     cpu = None
     if rank == 0 and not args.no_cpu:
-        gbs, cores, kind, sample = cpu_sample(h, args.ngf, args.cpu_seconds)
-        cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": cores, "kind": kind,
-               "sample": sample}
+        from carpet_b200.hierarchy import nested as nested_py
+        cpu = cpu_reference(nested_py(args.levels, args.npoints, ghost=3, buffer=9, order=5,
+                                      native=False),
+                            args.ngf, args.cpu_seconds / 3, 2, 1)
 
     serve = None
     if rank == 0 and not args.no_serve:
@@ -775,13 +758,11 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "fp_mode": args.fp, "ngf": args.ngf,
-                       "gf_groups": args.gf_groups, "gf_stagger": args.gf_stagger,
-                       "parallelism": "replicas" if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (~10 GB per step)",
-                       "bytes_per_step": int(bytes_step), "fine_points_per_step": int(points_step),
-                       "resident_gb": round(st.nbytes() / 1e9, 2),
-                       "tile_configs": {n: sorted(set(v.values())) for n, v in tuned.items()}},
+            "config": workload_config(args, bytes_step, points_step),
+            "fp_mode": args.fp, "gf_groups": args.gf_groups, "gf_stagger": args.gf_stagger,
+            "parallelism": "replicas" if world > 1 else "single GPU",
+            "resident_gb": round(st.nbytes() / 1e9, 2),
+            "tile_configs": {n: sorted(set(v.values())) for n, v in tuned.items()},
             "fine_points_per_s": round(fine_pts, 1),
             "pct_hbm_roof": round(100 * value / world / peak, 2),
             "pct_nominal_8tbs": round(100 * value / world / 8000.0, 2),

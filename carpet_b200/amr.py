@@ -36,7 +36,7 @@ import torch
 
 from .hierarchy import Hierarchy, npoints, size
 from .transfer import OP_LAGRANGE, VERTEX, Batch, Data, Graph, _arrays, _stream
-from . import _lib
+from . import _lib, bo
 import ctypes as C
 
 
@@ -149,7 +149,7 @@ class BergerOliger:
 
     # which pool holds timelevel tl of level l under rotation r
     def pool_index(self, r: int, tl: int) -> int:
-        return (tl - r) % self.st.ntl
+        return bo.pool_index(r, tl, self.st.ntl)
 
     def _tl(self, l, r, tl):
         return self.st.data[l][self.pool_index(r, tl)]
@@ -175,11 +175,7 @@ class BergerOliger:
             rf, rc = rots
             dst = self._tl(l, rf, 0)
             srcs = [self._tl(l - 1, rc, t) for t in range(st.ntl)]
-            # coarse timelevels at 0, -dt, -2dt; the fine level sits half a
-            # coarse step back (between timelevels) or on TL0
-            dtc = 1.0 / 64
-            times = [0.0, -dtc, -2 * dtc]
-            time = -dtc / 2 if ntl > 1 else 0.0
+            times, time = bo.prolong_times(ntl)
             b.add_many([(dst[g][p.dst_comp], [s[g][p.src_comp] for s in srcs], p.dstbox, p.srcbox)
                         for g in gfs for p in h.prolong[l]],
                        times, time, self.order_space, self.order_time, op=self.op, cent=self.cent)
@@ -204,26 +200,9 @@ class BergerOliger:
         return [self.batch(key, g) for g in range(self.groups)]
 
     def step_phases(self) -> List[tuple]:
-        """the phases of one coarse step, advancing the rotation state"""
-        L = self.L
-        nit = 2 ** (L - 1)
-        keys = []
-        for it in range(1, nit + 1):
-            for l in range(L):
-                every = 2 ** (L - 1 - l)
-                if (it - 1) % every == 0:
-                    self.rot[l] = (self.rot[l] + 1) % self.st.ntl  # cycle_all
-                    if l > 0:
-                        # odd substeps of level l fall between coarse times
-                        sub = ((it - 1) // every) % 2
-                        ntl = 3 if sub == 0 else 1
-                        keys.append(("prolong", l, (self.rot[l], self.rot[l - 1]), ntl))
-                    keys.append(("sync", l, (self.rot[l],), 1))
-            for l in range(L - 2, -1, -1):
-                if it % (2 ** (L - 1 - l)) == 0:
-                    keys.append(("restrict", l, (self.rot[l], self.rot[l + 1]), 1))
-                    keys.append(("sync", l, (self.rot[l],), 1))
-        return keys
+        """the phases of one coarse step, advancing the rotation state
+        (carpet_b200.bo.step_phases)"""
+        return bo.step_phases(self.L, self.st.ntl, self.rot)
 
     def autotune(self, keys, reps=2, stream=None):
         """tile configurations of every phase's prolongation kernels, chosen

@@ -774,8 +774,8 @@ struct cgx_batch {
   double *d_tmp = nullptr;
   size_t tmp_cap = 0;    // doubles
   std::vector<Desc> pdescs; // descs with the temporaries bound
-  // streams and events of the concurrent segment launch (created on first
-  // use, on the device current then)
+  // streams and events of the concurrent segment launch (created at upload,
+  // on the device current then)
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> ev; // ev[0] forks, ev[1 + k] joins side[k]
 };
@@ -967,6 +967,7 @@ int cgx_batch_stats(const cgx_batch *b, int64_t *npairs, int64_t *ntiles, int64_
   return CGX_OK;
 }
 
+static int ensure_side_streams(cgx_batch *b);
 int cgx_batch_upload(cgx_batch *b, void *stream) {
   if (!b) return fail(CGX_EINVAL, "null batch");
   cudaStream_t s = (cudaStream_t)stream;
@@ -1062,7 +1063,7 @@ int cgx_batch_upload(cgx_batch *b, void *stream) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(s); // host vectors are temporaries
     if (e != cudaSuccess) return cuda_fail(e, "descriptor upload");
   }
-  return CGX_OK;
+  return ensure_side_streams(b);
 }
 
 // The tile map's segments, one kernel each.  Pairs of a batch write
@@ -1073,51 +1074,76 @@ int cgx_batch_upload(cgx_batch *b, void *stream) {
 // stream of its own, forked from s and joined back into it (which also
 // works while s is being captured), and the time segment runs on s after
 // the join.  A batch with one such segment launches as one chain on s.
-static int launch_segments(cgx_batch *b, cudaStream_t s) {
+// indices of the non-empty segments before the time segment
+static int concurrent_segments(const cgx_batch *b, int *idx) {
   constexpr int TSEG = SEG_STREAM + SV_TIME;
-  static_assert(TSEG == NSEG - 1, "the time combination is the last segment");
-  int idx[NSEG], n = 0;
+  int n = 0;
   for (int i = 0; i < TSEG; ++i)
     if (b->seg[i + 1] > b->seg[i]) idx[n++] = i;
-  if (n <= 1)
-    return launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, b->seg, b->tma_cfg, b->d_counter,
-                      b->d_status, s);
-  const size_t nside = (size_t)n - 1;
-  cudaError_t e = cudaSuccess;
+  return n;
+}
+
+// The side streams and events of the concurrent launch, created when the
+// batch is uploaded (on the device current then), so that no launch -- a
+// captured one included -- creates any.
+static int ensure_side_streams(cgx_batch *b) {
+  int idx[NSEG];
+  const int n = concurrent_segments(b, idx);
+  const size_t nside = n > 1 ? (size_t)n - 1 : 0;
   while (b->side.size() < nside) {
     cudaStream_t x = nullptr;
-    e = cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking);
+    cudaError_t e = cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreateWithFlags");
     b->side.push_back(x);
   }
   while (b->ev.size() < nside + 1) {
     cudaEvent_t x = nullptr;
-    e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
+    cudaError_t e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
     if (e != cudaSuccess) return cuda_fail(e, "cudaEventCreateWithFlags");
     b->ev.push_back(x);
   }
+  return CGX_OK;
+}
+
+static int launch_segments(cgx_batch *b, cudaStream_t s) {
+  constexpr int TSEG = SEG_STREAM + SV_TIME;
+  static_assert(TSEG == NSEG - 1, "the time combination is the last segment");
+  int idx[NSEG];
+  const int n = concurrent_segments(b, idx);
+  if (n <= 1)
+    return launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, b->seg, b->tma_cfg, b->d_counter,
+                      b->d_status, s);
+  const size_t nside = (size_t)n - 1;
+  if (b->side.size() < nside || b->ev.size() < nside + 1)
+    return fail(CGX_EINVAL, "batch launch: the batch was not uploaded on this device");
   // a segment array in which only segment i is non-empty
   auto only = [&](int i, long long *sg) {
     for (int k = 0; k <= NSEG; ++k) sg[k] = k <= i ? b->seg[i] : b->seg[i + 1];
   };
-  e = cudaEventRecord(b->ev[0], s);
-  for (size_t k = 0; k < nside && e == cudaSuccess; ++k) e = cudaStreamWaitEvent(b->side[k], b->ev[0], 0);
-  if (e != cudaSuccess) return cuda_fail(e, "fork of the segment streams");
-  int rc = CGX_OK;
+  // fork: every side stream that has waited on ev[0] is joined below, also
+  // when a later fork step or a launch fails (a capture stays joined)
+  size_t forked = 0;
+  cudaError_t e = cudaEventRecord(b->ev[0], s);
+  while (e == cudaSuccess && forked < nside) {
+    e = cudaStreamWaitEvent(b->side[forked], b->ev[0], 0);
+    if (e == cudaSuccess) ++forked;
+  }
+  int rc = e != cudaSuccess ? cuda_fail(e, "fork of the segment streams") : CGX_OK;
   for (int j = 0; j < n && rc == CGX_OK; ++j) {
     long long sg[NSEG + 1];
     only(idx[j], sg);
     rc = launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, sg, b->tma_cfg, b->d_counter, b->d_status,
                     j == 0 ? s : b->side[j - 1]);
   }
-  // join every side stream, also after a failed launch
-  for (size_t k = 0; k < nside; ++k) {
+  // join every forked side stream, also after a failure
+  cudaError_t je = cudaSuccess;
+  for (size_t k = 0; k < forked; ++k) {
     cudaError_t r = cudaEventRecord(b->ev[1 + k], b->side[k]);
     if (r == cudaSuccess) r = cudaStreamWaitEvent(s, b->ev[1 + k], 0);
-    if (r != cudaSuccess && e == cudaSuccess) e = r;
+    if (r != cudaSuccess && je == cudaSuccess) je = r;
   }
   if (rc) return rc;
-  if (e != cudaSuccess) return cuda_fail(e, "join of the segment streams");
+  if (je != cudaSuccess) return cuda_fail(je, "join of the segment streams");
   if (b->seg[TSEG + 1] > b->seg[TSEG]) {
     long long sg[NSEG + 1];
     only(TSEG, sg);
@@ -1361,6 +1387,15 @@ extern "C" int cgx_transfer_pairs_noalloc(const cgx_pair *pairs, int npairs, voi
                 npairs, kNoAllocMaxPairs);
   if (npairs == 0) return CGX_OK;
   cudaStream_t s = (cudaStream_t)stream;
+  // The descriptors are copied from host memory that lives only for this
+  // call; a capture would record copies that read it after the call.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t ce = cudaStreamIsCapturing(s, &cap);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamIsCapturing");
+  if (cap != cudaStreamCaptureStatusNone)
+    return fail(CGX_EUNSUPPORTED, "cgx_transfer_pairs_noalloc cannot run inside a stream capture: "
+                                  "it copies its descriptors from host memory that the call does "
+                                  "not keep");
   unsigned char *base = nullptr;
   int rc = noalloc_scratch(&base);
   if (rc) return rc;
@@ -1408,6 +1443,26 @@ extern "C" int cgx_transfer_pairs_noalloc(const cgx_pair *pairs, int npairs, voi
   return g_fp_mode == CGX_FP_FMA
              ? klaunch_search_f1(d_descs, d_prefix, npairs, tiles, d_counter, d_status, s)
              : klaunch_search_f0(d_descs, d_prefix, npairs, tiles, d_counter, d_status, s);
+}
+
+// The status word the kernel of the last cgx_transfer_pairs_noalloc call on
+// the current device left in the fixed scratch (the next call clears it).
+// Waits for the stream, then reads the word into host memory; allocates
+// nothing.
+extern "C" int cgx_noalloc_check(void *stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned char *base = nullptr;
+  int rc = noalloc_scratch(&base);
+  if (rc) return rc;
+  int status = 0;
+  cudaError_t e = cudaMemcpyAsync(&status, base + kNoAllocCounterOff + sizeof(unsigned long long),
+                                  sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "status read-back");
+  if (status)
+    return fail(status, "cgx_transfer_pairs_noalloc: the kernel reported status %d (a bounded "
+                        "device wait gave up, or a descriptor had no tile routine)", status);
+  return CGX_OK;
 }
 
 // ============================================================== internal API

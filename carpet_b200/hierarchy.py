@@ -237,7 +237,8 @@ def schedule(h: Hierarchy, native: bool = True):
     """the sync / boundary-prolongation / restriction lists of every level,
     built by the library's C++ schedules (``native``) or by the Python
     restatement in this module (``_sync_pairs`` ...), which the tests compare"""
-    from . import sched
+    if native:
+        from . import sched
     for l, lev in enumerate(h.levels):
         h.sync[l] = sched.sync(lev.comps) if native else _sync_pairs(lev)
         if l > 0:

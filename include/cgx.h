@@ -270,11 +270,13 @@ int cgx_server_latencies(cgx_server *s, double *out_ms, int64_t n);
  * of under 0.5 MiB (room for CGX_NOALLOC_MAX_PAIRS descriptors) inside the
  * library's device image, which every GPU that loads the library holds until
  * the process exits; nothing is allocated.
- * The first call on a device looks up that array's device address, so make
- * the first call on each device outside any stream capture.  All calls share
- * the one array: calls whose kernels overlap on the GPU (other streams, or
- * other host threads) race and must be serialised by the caller.  Returns
- * CGX_EINVAL for more than CGX_NOALLOC_MAX_PAIRS pairs.  Asynchronous.
+ * The first call on a device looks up that array's device address.  The
+ * descriptors are copied from host memory that the call does not keep, so a
+ * call made while its stream is being captured returns CGX_EUNSUPPORTED.
+ * All calls share the one array: calls whose kernels overlap on the GPU
+ * (other streams, or other host threads) race and must be serialised by the
+ * caller.  Returns CGX_EINVAL for more than CGX_NOALLOC_MAX_PAIRS pairs.
+ * Asynchronous; cgx_noalloc_check reads the kernel's status afterwards.
  */
 #define CGX_NOALLOC_MAX_PAIRS 2048
 typedef struct cgx_pair {
@@ -290,6 +292,12 @@ typedef struct cgx_pair {
   int order_space, order_time;
 } cgx_pair;
 int cgx_transfer_pairs_noalloc(const cgx_pair *pairs, int npairs, void *stream);
+/* Waits for the stream and returns the status the last
+ * cgx_transfer_pairs_noalloc kernel on the current device left in the fixed
+ * scratch: CGX_OK, or CGX_EDEVICE when a bounded device wait gave up.
+ * Allocates nothing.  No counterpart in the reference (part of the
+ * no-allocation form above). */
+int cgx_noalloc_check(void *stream);
 
 /* device memory helpers for callers without their own allocator */
 int cgx_malloc(void **ptr, size_t bytes);

@@ -241,3 +241,94 @@ int cgxref_interpolate_eno_3d_3tl(const double *src1, double t1,
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// A list of box-pairs of one grid function through CarpetLib's own local
+// transfer path, data<T>::transfer_time (CarpetLib/src/data.cc:486-534),
+// with the loop over the pairs in C++ so that the CPU baseline times the
+// operators rather than the caller: for each pair, with ntl > 1 one
+// temporary per timelevel over the destination box (allocated and freed per
+// call, as data.cc:506-520 does), the spatial operator into each, then
+// time_interpolate into the destination (data.cc:1183-1259); with ntl == 1
+// the spatial operator straight into the destination.  The spatial operator
+// follows transfer_p_r (data.cc:537-556): copy_3d without call_operator
+// (copy_from_innerloop, data.cc:433-462), prolongate_3d_rf2<order_space>
+// and restrict_3d_rf2 through call_operator (data.cc:600-613, 1039-1046).
+//
+// kind 0 = copy, 1 = vertex-centred Lagrange prolongation, 2 = injection.
+// Arrays are {data, padext[3], bbox[9]}; src holds npairs * ntl arrays,
+// pair-major.
+struct cgxref_arr {
+  double *data;
+  int padext[3];
+  int bbox[9];
+};
+
+namespace {
+ivect3 shape_of(const int *b) {
+  return ivect3((b[3] - b[0]) / b[6] + 1, (b[4] - b[1]) / b[7] + 1, (b[5] - b[2]) / b[8] + 1);
+}
+op_t vc_operator(int order) {
+  switch (order) {
+  case 1: return &prolongate_3d_rf2<double, 1>;
+  case 3: return &prolongate_3d_rf2<double, 3>;
+  case 5: return &prolongate_3d_rf2<double, 5>;
+  case 7: return &prolongate_3d_rf2<double, 7>;
+  case 9: return &prolongate_3d_rf2<double, 9>;
+  case 11: return &prolongate_3d_rf2<double, 11>;
+  }
+  throw std::runtime_error("no vertex-centred stencil of this order");
+}
+// transfer_p_r of one timelevel into (out, outpad, outbox)
+void spatial(int kind, int order, const cgxref_arr &src, double *out, ivect3 const &outpad,
+             ibbox3 const &outbox, ibbox3 const &dstbox, ibbox3 const &srcbox) {
+  ivect3 const spad = iv(src.padext), sext = shape_of(src.bbox);
+  ibbox3 const sbb = ib(src.bbox);
+  ivect3 const oext = outbox.sizes();
+  switch (kind) {
+  case 0:
+    copy_3d<double>(src.data, spad, sext, out, outpad, oext, sbb, outbox, srcbox, dstbox, nullptr);
+    return;
+  case 1:
+    call_operator(vc_operator(order), src.data, spad, sext, out, outpad, oext, sbb, outbox, srcbox,
+                  dstbox);
+    return;
+  case 2:
+    call_operator(&restrict_3d_rf2<double>, src.data, spad, sext, out, outpad, oext, sbb, outbox,
+                  srcbox, dstbox);
+    return;
+  }
+  throw std::runtime_error("unknown transfer kind");
+}
+} // namespace
+
+extern "C" int cgxref_transfer_pairs(int kind, int order_space, int npairs, const cgxref_arr *dst,
+                                     const cgxref_arr *src, int ntl, const int *dstboxes,
+                                     const int *srcboxes, const double *times, double time) {
+  return guarded([&] {
+    if (ntl < 1 || ntl > 3) throw std::runtime_error("1 to 3 timelevels");
+    for (int p = 0; p < npairs; ++p) {
+      const cgxref_arr &d = dst[p];
+      ibbox3 const dstbox = ib(dstboxes + 9 * p), srcbox = ib(srcboxes + 9 * p);
+      ibbox3 const dbb = ib(d.bbox);
+      ivect3 const dpad = iv(d.padext), dext = shape_of(d.bbox);
+      if (ntl == 1) {
+        spatial(kind, order_space, src[(size_t)p * ntl], d.data, dpad, dbb, dstbox, srcbox);
+        continue;
+      }
+      ivect3 const tsz = dstbox.sizes();
+      size_t const n = (size_t)tsz[0] * tsz[1] * tsz[2];
+      double *tmp[3] = {nullptr, nullptr, nullptr};
+      for (int t = 0; t < ntl; ++t) tmp[t] = new double[n];
+      for (int t = 0; t < ntl; ++t)
+        spatial(kind, order_space, src[(size_t)p * ntl + t], tmp[t], tsz, dstbox, dstbox, srcbox);
+      if (ntl == 2)
+        interpolate_3d_2tl<double>(tmp[0], times[0], tmp[1], times[1], tsz, tsz, d.data, time, dpad,
+                                   dext, dstbox, dbb, dstbox, dstbox, nullptr);
+      else
+        interpolate_3d_3tl<double>(tmp[0], times[0], tmp[1], times[1], tmp[2], times[2], tsz, tsz,
+                                   d.data, time, dpad, dext, dstbox, dbb, dstbox, dstbox, nullptr);
+      for (int t = 0; t < ntl; ++t) delete[] tmp[t];
+    }
+  });
+}

@@ -10,9 +10,11 @@ in allocated memory.
 
 This test calls that entry point through the C-ABI twice in a row and checks
 each result bit for bit against the ordinary per-box entry point
-(cgx_transfer) on the same inputs -- the same bar as every other parity test
--- and checks that an over-long pair list is refused.  It sits in the last
-collected test file and passes both alone and after the other tests.
+(cgx_transfer) and against the oracle on the same inputs -- the same bar as
+every other parity test -- reads the kernel's status back through
+cgx_noalloc_check, and checks that an over-long pair list and a call inside a
+stream capture are refused.  It sits in the last collected test file and
+passes both alone and after the other tests.
 """
 import ctypes as C
 
@@ -20,7 +22,7 @@ import numpy as np
 import pytest
 
 from oracle import cases
-from oracle.binding import CELL, OP_ENO, OP_LAGRANGE, OP_LAGRANGE_MONOTONE, VERTEX
+from oracle.binding import CELL, OP_ENO, OP_LAGRANGE, OP_LAGRANGE_MONOTONE, VERTEX, Port
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
@@ -76,9 +78,10 @@ def lib():
 def _run(lib, seed, n):
     from carpet_b200._lib import box9
     cgx_array, cgx_pair = _structs()
-    lib.cgx_set_fp_mode(1)
+    lib.cgx_set_fp_mode(0)  # the reference's operation order, two roundings per multiply-add
+    port = Port()
     pairs = (cgx_pair * n)()
-    keep, ref_dsts, na_dsts = [], [], []
+    keep, ref_dsts, na_dsts, oracle_dsts = [], [], [], []
     t0, dt = 0.5, 0.125
     for i, (op, cent, c, order) in enumerate(_make_pairs(seed, n)):
         ntl = 1 + i % 3
@@ -123,34 +126,58 @@ def _run(lib, seed, n):
         rc = lib.cgx_transfer(op, cent, C.byref(dref), sarr, ts, 3, box9(c["reg"]),
                               box9(c["srcbbox"]), None, time, order, ot, None)
         assert rc == 0, lib.cgx_last_error()
+        # and the oracle on the same arguments
+        want = c["dst"].copy()
+        port.transfer(op, cent, want, c["dstbbox"], srcs_np, c["srcbbox"], times, c["reg"],
+                      c["srcbbox"], time, order, ot)
+        oracle_dsts.append(want)
     torch.cuda.synchronize()
-    return pairs, keep, ref_dsts, na_dsts
+    return pairs, keep, ref_dsts, na_dsts, oracle_dsts
 
 
-def test_noalloc_matches_per_box_twice(lib):
-    pairs, keep, ref_dsts, na_dsts = _run(lib, 777, 48)
+def test_noalloc_matches_per_box_and_oracle_twice(lib):
+    pairs, keep, ref_dsts, na_dsts, oracle_dsts = _run(lib, 777, 48)
     n = len(ref_dsts)
     for call in range(2):
         for d, init in na_dsts:
             d.copy_(init)
         rc = lib.cgx_transfer_pairs_noalloc(pairs, n, None)
         assert rc == 0, lib.cgx_last_error()
-        torch.cuda.synchronize()
-        for i, ((d, _), r) in enumerate(zip(na_dsts, ref_dsts)):
+        assert lib.cgx_noalloc_check(None) == 0, lib.cgx_last_error()
+        for i, ((d, _), r, o) in enumerate(zip(na_dsts, ref_dsts, oracle_dsts)):
             a = d.cpu().numpy().view(np.uint64)
-            b = r.cpu().numpy().view(np.uint64)
-            assert np.array_equal(a, b), (call, i)
+            assert np.array_equal(a, r.cpu().numpy().view(np.uint64)), (call, i, "per box")
+            assert np.array_equal(a, o.view(np.uint64)), (call, i, "oracle")
 
 
 def test_noalloc_second_list_reuses_scratch(lib):
     """a different, shorter list right after: the shared scratch keeps the
     previous call's contents, and the counter must start from zero again"""
-    pairs, keep, ref_dsts, na_dsts = _run(lib, 778, 17)
+    pairs, keep, ref_dsts, na_dsts, oracle_dsts = _run(lib, 778, 17)
     rc = lib.cgx_transfer_pairs_noalloc(pairs, len(ref_dsts), None)
     assert rc == 0, lib.cgx_last_error()
-    torch.cuda.synchronize()
-    for (d, _), r in zip(na_dsts, ref_dsts):
+    assert lib.cgx_noalloc_check(None) == 0, lib.cgx_last_error()
+    for (d, _), r, o in zip(na_dsts, ref_dsts, oracle_dsts):
         assert np.array_equal(d.cpu().numpy().view(np.uint64), r.cpu().numpy().view(np.uint64))
+        assert np.array_equal(d.cpu().numpy().view(np.uint64), o.view(np.uint64))
+
+
+def test_noalloc_refuses_stream_capture(lib):
+    """the descriptors come from host memory that the call does not keep, so
+    a call on a stream under capture is refused and the capture ends cleanly"""
+    pairs, keep, ref_dsts, na_dsts, _ = _run(lib, 780, 4)
+    s = torch.cuda.Stream()
+    sp = C.c_void_p(s.cuda_stream)
+    lib.cgx_graph_begin.argtypes = [C.c_void_p]
+    lib.cgx_graph_end.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    lib.cgx_graph_destroy.argtypes = [C.c_void_p]
+    assert lib.cgx_graph_begin(sp) == 0, lib.cgx_last_error()
+    rc = lib.cgx_transfer_pairs_noalloc(pairs, len(ref_dsts), sp)
+    g = C.c_void_p()
+    assert lib.cgx_graph_end(sp, C.byref(g)) == 0, lib.cgx_last_error()
+    lib.cgx_graph_destroy(g)
+    assert rc == 2
+    assert b"capture" in lib.cgx_last_error()
 
 
 def test_noalloc_rejects_too_many_pairs(lib):
