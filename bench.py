@@ -92,6 +92,12 @@ def parse():
                    help="grid-function groups whose phase chains run on separate streams")
     p.add_argument("--gf-stagger", type=int, default=GF_STAGGER,
                    help="phases by which each further grid-function group starts after the first")
+    p.add_argument("--chain", type=int, default=0, choices=[0, 1],
+                   help="1: each coarse step as one chain launch (one persistent kernel with "
+                        "per-grid-function dependency counters) instead of one launch per phase")
+    p.add_argument("--max-ctas", type=int, nargs=2, default=[0, 0], metavar=("TMA", "STREAM"),
+                   help="CTAs per SM of the TMA prolongation and the streaming kernels (0: all that "
+                        "fit); below the limit, the grid-function groups' kernels share the SMs")
     p.add_argument("--moving", action="store_true",
                    help="add the moving-box section (~80 GB on the device, minutes)")
     return p.parse_args()
@@ -512,8 +518,10 @@ def main():
     h = nested(args.levels, args.npoints, ghost=3, buffer=9, order=5)
     st = Storage(h, args.ngf, 3)
     fill_storage(st, h, seed=1 + rank)
+    if args.chain:
+        args.gf_groups, args.gf_stagger = 1, 0
     bo = BergerOliger(h, st, order_space=5, order_time=2, groups=args.gf_groups,
-                      stagger=args.gf_stagger)
+                      stagger=args.gf_stagger, chain=bool(args.chain), max_ctas=args.max_ctas)
     steps3 = [bo.step_phases() for _ in range(3)]  # the rotation repeats every 3 steps
     for keys in steps3:
         for k in keys:
@@ -525,7 +533,7 @@ def main():
             for k in keys:
                 tuned_by_key[k] = {v: args.tile_config for v in range(40)}
         tuned = {"all": {0: args.tile_config}}
-    elif not args.no_tune:
+    elif not args.no_tune and not args.chain:
         for keys in steps3:
             for k, v in bo.autotune(keys, reps=5).items():
                 tuned_by_key[k] = v
@@ -539,9 +547,14 @@ def main():
     from carpet_b200.bo import workload_totals
     if (int(bytes_step), int(points_step)) != tuple(int(x) for x in workload_totals(h, args.ngf)):
         raise RuntimeError("algorithmic byte counts of the library and the schedule differ")
-    kernels_step = sum(s["kernels"] for s in stats) / 3
+    kernels_step = 1 if args.chain else sum(s["kernels"] for s in stats) / 3
     stream = torch.cuda.Stream()
     torch.cuda.synchronize()
+    if args.chain:
+        for keys in steps3:
+            c = bo.chain(keys, stream)  # built and uploaded outside the captures
+            if c.stats()["bytes"] != bytes_step:
+                raise RuntimeError("the chain's algorithmic bytes differ from the step's")
 
     # capture the three step variants as graphs
     graphs = []
@@ -570,6 +583,8 @@ def main():
     ms = replicas.max_over_ranks(e0.elapsed_time(e1) / args.steps)
     for b in bo.batches.values():
         b.check(stream)
+    for c in bo.chains.values():
+        c.check(stream)
     value = replicas.job_throughput(bytes_step, world, ms) / 1e9
     fine_pts = replicas.job_throughput(points_step, world, ms)
 
@@ -660,7 +675,7 @@ def main():
             for p, q in zip(la, lb):
                 q.copy_(p)
         boB = BergerOliger(h, stB, order_space=5, order_time=2, groups=args.gf_groups,
-                           stagger=args.gf_stagger)
+                           stagger=args.gf_stagger, chain=bool(args.chain), max_ctas=args.max_ctas)
         stepsB = [boB.step_phases() for _ in range(3)]
         for keys in stepsB:
             for k in keys:
@@ -670,6 +685,8 @@ def main():
                     b.upload()
         graphsB = []
         for keys in stepsB:
+            if args.chain:
+                boB.chain(keys, stream)  # built and uploaded outside the capture
             g = cb.Graph()
             with g.capture(stream):
                 boB.run(keys, stream)
@@ -720,6 +737,8 @@ def main():
                "pipelining": "two device copies alternate; copy-in, kernels, copy-out on three streams"}
         for b in boB.batches.values():
             b.check(stream)
+        for c in boB.chains.values():
+            c.check(stream)
         del graphsB
 
     cpu = None

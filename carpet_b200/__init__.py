@@ -14,7 +14,7 @@ from __future__ import annotations
 import importlib
 
 _TRANSFER_NAMES = ("CELL", "OP_COPY", "OP_ENO", "OP_LAGRANGE", "OP_NONE", "OP_RESTRICT", "OP_SYNC",
-                   "OP_WENO", "VERTEX", "Batch", "CgxError", "Data", "Graph", "copy_data",
+                   "OP_WENO", "VERTEX", "Batch", "Chain", "CgxError", "Data", "Graph", "copy_data",
                    "set_fp_mode", "set_restriction", "transfer_data")
 
 __all__ = list(_TRANSFER_NAMES)

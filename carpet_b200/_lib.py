@@ -77,6 +77,14 @@ lib.cgx_graph_destroy.argtypes = [C.c_void_p]
 lib.cgx_find_source_timelevel.argtypes = [_P(C.c_double), C.c_int, C.c_double, C.c_int, C.c_int,
                                           _P(C.c_int), _P(C.c_int)]
 lib.cgx_stream_sync.argtypes = [C.c_void_p]
+lib.cgx_batch_set_group.argtypes = [C.c_void_p, C.c_int]
+lib.cgx_batch_set_max_ctas.argtypes = [C.c_void_p, C.c_int, C.c_int]
+lib.cgx_chain_create.argtypes = [_P(C.c_void_p)]
+lib.cgx_chain_destroy.argtypes = [C.c_void_p]
+lib.cgx_chain_add.argtypes = [C.c_void_p, C.c_void_p]
+for fn in ("cgx_chain_upload", "cgx_chain_launch", "cgx_chain_check"):
+    getattr(lib, fn).argtypes = [C.c_void_p, C.c_void_p]
+lib.cgx_chain_stats.argtypes = [C.c_void_p] + [_P(C.c_int64)] * 4
 
 
 def check(rc: int):

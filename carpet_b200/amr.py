@@ -35,7 +35,7 @@ import numpy as np
 import torch
 
 from .hierarchy import Hierarchy, npoints, size
-from .transfer import OP_LAGRANGE, VERTEX, Batch, Data, Graph, _arrays, _stream
+from .transfer import OP_LAGRANGE, VERTEX, Batch, Chain, Data, Graph, _arrays, _stream
 from . import _lib, bo
 import ctypes as C
 
@@ -133,9 +133,19 @@ class BergerOliger:
     """Transfer phases of one coarse step of a nested hierarchy."""
 
     def __init__(self, h: Hierarchy, st: Storage, order_space=5, order_time=2,
-                 op=OP_LAGRANGE, cent=VERTEX, groups: int = 1, stagger: int = 0):
+                 op=OP_LAGRANGE, cent=VERTEX, groups: int = 1, stagger: int = 0,
+                 chain: bool = False, max_ctas=(0, 0)):
+        """``chain``: run a step's phases as one chain (one persistent
+        launch, carpet_b200.transfer.Chain) instead of one launch per phase;
+        needs groups == 1 (the chain overlaps the grid functions itself)"""
         if not 1 <= groups <= st.ngf:
             raise ValueError("groups must lie in 1..ngf")
+        if chain and groups != 1:
+            raise ValueError("a chained step runs its grid functions in one launch: groups must be 1")
+        self.use_chain = chain
+        # CTAs per SM of every batch's TMA / streaming kernels (0: all that fit)
+        self.max_ctas = tuple(max_ctas)
+        self.chains: Dict[tuple, Chain] = {}
         if stagger < 0:
             raise ValueError("stagger must not be negative")
         self.h, self.st = h, st
@@ -165,27 +175,32 @@ class BergerOliger:
         b = Batch()
         h, st = self.h, self.st
         gfs = self.gfs(grp)
-        if kind == "sync":
-            r, = rots
-            arrs = self._tl(l, r, 0)
-            b.add_many([(arrs[g][p.dst_comp], [arrs[g][p.src_comp]], p.dstbox, p.srcbox)
-                        for g in gfs for p in h.sync[l]],
-                       [0.0], 0.0, 1, 0, op=self.op, cent=self.cent)
-        elif kind == "prolong":
-            rf, rc = rots
-            dst = self._tl(l, rf, 0)
-            srcs = [self._tl(l - 1, rc, t) for t in range(st.ntl)]
-            times, time = bo.prolong_times(ntl)
-            b.add_many([(dst[g][p.dst_comp], [s[g][p.src_comp] for s in srcs], p.dstbox, p.srcbox)
-                        for g in gfs for p in h.prolong[l]],
-                       times, time, self.order_space, self.order_time, op=self.op, cent=self.cent)
-        elif kind == "restrict":
-            rc, rf = rots
-            dst = self._tl(l, rc, 0)
-            src = self._tl(l + 1, rf, 0)
-            b.add_many([(dst[g][p.dst_comp], [src[g][p.src_comp]], p.dstbox, p.srcbox)
-                        for g in gfs for p in h.restrict[l + 1]],
-                       [0.0], 0.0, self.order_space, 0, op=self.op, cent=self.cent)
+        # one dependency group per grid function (a chain keeps each grid
+        # function's phases in order and lets the others overlap)
+        for g in gfs:
+            b.set_group(g)
+            if kind == "sync":
+                r, = rots
+                arrs = self._tl(l, r, 0)
+                b.add_many([(arrs[g][p.dst_comp], [arrs[g][p.src_comp]], p.dstbox, p.srcbox)
+                            for p in h.sync[l]],
+                           [0.0], 0.0, 1, 0, op=self.op, cent=self.cent)
+            elif kind == "prolong":
+                rf, rc = rots
+                dst = self._tl(l, rf, 0)
+                srcs = [self._tl(l - 1, rc, t) for t in range(st.ntl)]
+                times, time = bo.prolong_times(ntl)
+                b.add_many([(dst[g][p.dst_comp], [s[g][p.src_comp] for s in srcs], p.dstbox, p.srcbox)
+                            for p in h.prolong[l]],
+                           times, time, self.order_space, self.order_time, op=self.op, cent=self.cent)
+            elif kind == "restrict":
+                rc, rf = rots
+                dst = self._tl(l, rc, 0)
+                src = self._tl(l + 1, rf, 0)
+                b.add_many([(dst[g][p.dst_comp], [src[g][p.src_comp]], p.dstbox, p.srcbox)
+                            for p in h.restrict[l + 1]],
+                           [0.0], 0.0, self.order_space, 0, op=self.op, cent=self.cent)
+        b.set_max_ctas(*self.max_ctas)
         b.upload()
         return b
 
@@ -225,6 +240,15 @@ class BergerOliger:
                 b.set_config(config)
                 b.upload(stream)
 
+    def chain(self, keys, stream=None) -> Chain:
+        """the phases as one chain, built and uploaded on first use"""
+        k = tuple(keys)
+        if k not in self.chains:
+            c = Chain([self.batch(x) for x in keys])
+            c.upload(stream)
+            self.chains[k] = c
+        return self.chains[k]
+
     def run(self, keys, stream=None, per_box=False, stagger=None):
         """launch the phases in order; with several groups, group g's chain
         runs on its own stream, forked from and joined back into stream
@@ -239,6 +263,9 @@ class BergerOliger:
                 b.launch_per_box(s)
             else:
                 b.launch(s)
+        if self.use_chain and not per_box:
+            self.chain(keys, stream).launch(stream)
+            return
         if self.groups == 1:
             for k in keys:
                 launch(self.batch(k), stream)

@@ -37,6 +37,29 @@ def _deps():
         os.path.join(os.path.dirname(HERE), "include", "cgx.h"), __file__]
 
 
+def _includes(path, seen=None):
+    """the local headers a source includes, transitively"""
+    import re
+    seen = set() if seen is None else seen
+    try:
+        text = open(path).read()
+    except OSError:
+        return seen
+    for inc in re.findall(r'#include\s+"([^"]+)"', text):
+        q = os.path.normpath(os.path.join(os.path.dirname(path), inc))
+        if q not in seen and os.path.exists(q):
+            seen.add(q)
+            _includes(q, seen)
+    return seen
+
+
+def _stale(src: str, obj: str) -> bool:
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(p) > t for p in [src, __file__, *_includes(src)])
+
+
 def up_to_date() -> bool:
     if not os.path.exists(LIB):
         return False
@@ -52,6 +75,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
     def compile_one(src):
         obj = os.path.join(OBJDIR, os.path.basename(src)[:-3] + ".o")
+        if not force and not _stale(src, obj):
+            return obj, ""
         cmd = [cc, *ARCH, *FLAGS, "-c", src, "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

@@ -14,10 +14,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -701,9 +703,22 @@ const TmaLaunch kTmaLaunch[2][2][TMA_NCFG] = {{CGX_TMA_ROW(0, 0), CGX_TMA_ROW(0,
                                               {CGX_TMA_ROW(1, 0), CGX_TMA_ROW(1, 1)}};
 #undef CGX_TMA_ROW
 
+int launch_map_capped(int fp, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
+                      const long long seg[NSEG + 1], const int *cfg, unsigned long long *counter, int *status,
+                      cudaStream_t s);
+// with the batch's CTA caps in force for these launches only
 int launch_map(int fp, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
                const long long seg[NSEG + 1], const int *cfg, unsigned long long *counter, int *status,
-               cudaStream_t s) {
+               cudaStream_t s, const int *caps = nullptr) {
+  g_cta_cap[0] = caps ? caps[0] : 0;
+  g_cta_cap[1] = caps ? caps[1] : 0;
+  const int rc = launch_map_capped(fp, d, maps, tmap, seg, cfg, counter, status, s);
+  g_cta_cap[0] = g_cta_cap[1] = 0;
+  return rc;
+}
+int launch_map_capped(int fp, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
+                      const long long seg[NSEG + 1], const int *cfg, unsigned long long *counter, int *status,
+                      cudaStream_t s) {
   const bool f = fp == CGX_FP_FMA;
   for (int i = 0; i < NSEG; ++i) {
     const long long n = seg[i + 1] - seg[i];
@@ -778,6 +793,11 @@ struct cgx_batch {
   // on the device current then)
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> ev; // ev[0] forks, ev[1 + k] joins side[k]
+  // CTAs per SM of the TMA and the streaming kernels (0: as many as fit)
+  int max_ctas[2] = {0, 0};
+  // dependency group of every descriptor (cgx_batch_set_group; the chain)
+  int cur_group = 0;
+  std::vector<int> group;
 };
 
 namespace {
@@ -790,6 +810,7 @@ void batch_push(cgx_batch *b, const Desc &d, long long bytes, long long points, 
   b->high.push_back(d.kind == K_PROLONG_VC && d.order >= 7);
   b->tdst.push_back(tdst);
   b->tsrc.push_back(tsrc);
+  b->group.push_back(b->cur_group);
 }
 void batch_add_built(cgx_batch *b, const Built &x) {
   if (!x.nst) {
@@ -918,8 +939,25 @@ int cgx_batch_clear(cgx_batch *b) {
   b->high.clear();
   b->tdst.clear();
   b->tsrc.clear();
+  b->group.clear();
+  b->cur_group = 0;
   b->tmp_elems = 0;
   b->nstage1 = 0;
+  return CGX_OK;
+}
+
+int cgx_batch_set_max_ctas(cgx_batch *b, int tma_per_sm, int stream_per_sm) {
+  if (!b) return fail(CGX_EINVAL, "null batch");
+  if (tma_per_sm < 0 || stream_per_sm < 0) return fail(CGX_EINVAL, "CTA caps must not be negative");
+  b->max_ctas[0] = tma_per_sm;
+  b->max_ctas[1] = stream_per_sm;
+  return CGX_OK;
+}
+
+int cgx_batch_set_group(cgx_batch *b, int group) {
+  if (!b) return fail(CGX_EINVAL, "null batch");
+  if (group < 0) return fail(CGX_EINVAL, "group must not be negative");
+  b->cur_group = group;
   return CGX_OK;
 }
 
@@ -1112,7 +1150,7 @@ static int launch_segments(cgx_batch *b, cudaStream_t s) {
   const int n = concurrent_segments(b, idx);
   if (n <= 1)
     return launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, b->seg, b->tma_cfg, b->d_counter,
-                      b->d_status, s);
+                      b->d_status, s, b->max_ctas);
   const size_t nside = (size_t)n - 1;
   if (b->side.size() < nside || b->ev.size() < nside + 1)
     return fail(CGX_EINVAL, "batch launch: the batch was not uploaded on this device");
@@ -1133,7 +1171,7 @@ static int launch_segments(cgx_batch *b, cudaStream_t s) {
     long long sg[NSEG + 1];
     only(idx[j], sg);
     rc = launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, sg, b->tma_cfg, b->d_counter, b->d_status,
-                    j == 0 ? s : b->side[j - 1]);
+                    j == 0 ? s : b->side[j - 1], b->max_ctas);
   }
   // join every forked side stream, also after a failure
   cudaError_t je = cudaSuccess;
@@ -1147,7 +1185,8 @@ static int launch_segments(cgx_batch *b, cudaStream_t s) {
   if (b->seg[TSEG + 1] > b->seg[TSEG]) {
     long long sg[NSEG + 1];
     only(TSEG, sg);
-    rc = launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, sg, b->tma_cfg, b->d_counter, b->d_status, s);
+    rc = launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, sg, b->tma_cfg, b->d_counter, b->d_status, s,
+                    b->max_ctas);
   }
   return rc;
 }
@@ -1337,6 +1376,210 @@ int cgx_stream_sync(void *stream) {
 
 } // extern "C"
 
+
+// ============================================================== chain
+// A sequence of batches run as ONE persistent launch (cgx_chain.cuh): the
+// tiles of batch j wait, group by group, for the previous batch of their
+// group.  The descriptors, tensor maps and tile list are built here from the
+// batches' host-side pairs.
+struct cgx_chain {
+  std::vector<cgx_batch *> batches;
+  int order = -1; // vertex-centred prolongation order of every prolongation pair
+  int fp_mode = CGX_FP_EXACT;
+  Desc *d_descs = nullptr;
+  CUtensorMap *d_maps = nullptr;
+  ChainTile *d_tiles = nullptr;
+  unsigned *d_need = nullptr, *d_done = nullptr;
+  unsigned long long *d_ctl = nullptr;
+  int *d_status = nullptr;
+  long long ntiles = 0;
+  int ncounters = 0;
+  long long pairs = 0, points = 0, bytes = 0;
+};
+
+namespace {
+void chain_free(cgx_chain *c) {
+  cudaFree(c->d_descs);
+  cudaFree(c->d_maps);
+  cudaFree(c->d_tiles);
+  cudaFree(c->d_need);
+  cudaFree(c->d_done);
+  cudaFree(c->d_ctl);
+  cudaFree(c->d_status);
+  c->d_descs = nullptr;
+  c->d_maps = nullptr;
+  c->d_tiles = nullptr;
+  c->d_need = c->d_done = nullptr;
+  c->d_ctl = nullptr;
+  c->d_status = nullptr;
+  c->ntiles = 0;
+  c->ncounters = 0;
+}
+} // namespace
+
+extern "C" {
+
+int cgx_chain_create(cgx_chain **out) {
+  if (!out) return fail(CGX_EINVAL, "null chain");
+  *out = new cgx_chain();
+  return CGX_OK;
+}
+
+int cgx_chain_destroy(cgx_chain *c) {
+  if (!c) return CGX_OK;
+  chain_free(c);
+  delete c;
+  return CGX_OK;
+}
+
+int cgx_chain_add(cgx_chain *c, cgx_batch *b) {
+  if (!c || !b) return fail(CGX_EINVAL, "null chain or batch");
+  c->batches.push_back(b);
+  return CGX_OK;
+}
+
+int cgx_chain_upload(cgx_chain *c, void *stream) {
+  if (!c) return fail(CGX_EINVAL, "null chain");
+  cudaStream_t s = (cudaStream_t)stream;
+  constexpr int CFG = 1; // the chain kernel's prolongation tile configuration
+  const TmaCfg &cfg = TMA_CFGS[CFG];
+  std::vector<Desc> hd;
+  std::vector<CUtensorMap> hm;
+  std::vector<ChainTile> ht;
+  std::vector<unsigned> need;
+  int order = -1;
+  long long pairs = 0, points = 0, bytes = 0;
+  std::map<int, int> last_of_group; // group -> its latest counter
+  for (size_t j = 0; j < c->batches.size(); ++j) {
+    const cgx_batch *b = c->batches[j];
+    if (b->nstage1)
+      return fail(CGX_EUNSUPPORTED, "chain: batch %zu has transfers through temporaries", j);
+    // this batch's descriptors group by group
+    std::map<int, std::vector<int>> by_group;
+    for (size_t i = 0; i < b->descs.size(); ++i) by_group[b->group[i]].push_back((int)i);
+    for (auto &kv : by_group) {
+      const int counter = (int)need.size();
+      auto it = last_of_group.find(kv.first);
+      const int dep = it == last_of_group.end() ? -1 : it->second;
+      last_of_group[kv.first] = counter;
+      unsigned count = 0;
+      for (int i : kv.second) {
+        Desc d = b->descs[i];
+        long long nt = 0;
+        CUtensorMap maps[3] = {};
+        if (d.kind == K_PROLONG_VC) {
+          const bool time_ok = d.ntl == 1 || (d.ntl == 3 && d.tkind == T_QUAD);
+          if (!time_ok || (d.order != 1 && d.order != 3 && d.order != 5))
+            return fail(CGX_EUNSUPPORTED,
+                        "chain: batch %zu pair %d: only vertex-centred orders 1/3/5 with one "
+                        "timelevel or quadratic time interpolation",
+                        j, i);
+          if (order >= 0 && d.order != order)
+            return fail(CGX_EUNSUPPORTED, "chain: prolongation orders %d and %d mixed", order, d.order);
+          order = d.order;
+          nt = prolong_tiles(d, cfg.pyc, cfg.pz);
+          if (nt <= 0 || nt >= (1LL << 31) || !encode_tma_maps(d, maps))
+            return fail(CGX_EUNSUPPORTED,
+                        "chain: batch %zu pair %d: the source arrays cannot be staged by TMA "
+                        "(16-byte aligned base, even row and plane pitch)",
+                        j, i);
+        } else if ((d.kind == K_COPY && d.ntl == 1) || d.kind == K_RESTRICT_VC) {
+          nt = b->ntiles[i];
+        } else {
+          return fail(CGX_EUNSUPPORTED,
+                      "chain: batch %zu pair %d: only vertex-centred prolongation, one-timelevel "
+                      "copies and injection run in the chain kernel",
+                      j, i);
+        }
+        const int di = (int)hd.size();
+        hd.push_back(d);
+        for (int t = 0; t < 3; ++t) hm.push_back(maps[t]);
+        for (long long k = 0; k < nt; ++k) ht.push_back(ChainTile{di, (int)k, counter, dep});
+        count += (unsigned)nt;
+        ++pairs;
+        points += b->points[i];
+        bytes += b->bytes[i];
+      }
+      need.push_back(count);
+    }
+  }
+  if (hd.size() >= (size_t)INT_MAX || ht.size() >= (size_t)INT_MAX)
+    return fail(CGX_EINVAL, "chain: too many pairs or tiles");
+  chain_free(c);
+  const size_t nd = std::max<size_t>(hd.size(), 1), nt = std::max<size_t>(ht.size(), 1),
+               nc = std::max<size_t>(need.size(), 1);
+  cudaError_t e = cudaMalloc(&c->d_descs, nd * sizeof(Desc));
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_maps, 3 * nd * sizeof(CUtensorMap));
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_tiles, nt * sizeof(ChainTile));
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_need, nc * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_done, nc * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_ctl, CHAIN_CTL_WORDS * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_status, sizeof(int));
+  if (e != cudaSuccess) {
+    chain_free(c);
+    return cuda_fail(e, "cudaMalloc (chain)");
+  }
+  if (!hd.empty()) e = cudaMemcpyAsync(c->d_descs, hd.data(), hd.size() * sizeof(Desc), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && !hm.empty())
+    e = cudaMemcpyAsync(c->d_maps, hm.data(), hm.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && !ht.empty())
+    e = cudaMemcpyAsync(c->d_tiles, ht.data(), ht.size() * sizeof(ChainTile), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && !need.empty())
+    e = cudaMemcpyAsync(c->d_need, need.data(), need.size() * sizeof(unsigned), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_done, 0, nc * sizeof(unsigned), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_ctl, 0, CHAIN_CTL_WORDS * sizeof(unsigned long long), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_status, 0, sizeof(int), s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s); // the host vectors are temporaries
+  if (e != cudaSuccess) {
+    chain_free(c);
+    return cuda_fail(e, "chain upload");
+  }
+  c->ntiles = (long long)ht.size();
+  c->ncounters = (int)need.size();
+  c->order = order < 0 ? 5 : order;
+  c->fp_mode = g_fp_mode;
+  c->pairs = pairs;
+  c->points = points;
+  c->bytes = bytes;
+  return CGX_OK;
+}
+
+int cgx_chain_launch(cgx_chain *c, void *stream) {
+  if (!c) return fail(CGX_EINVAL, "null chain");
+  if (c->ntiles == 0) return CGX_OK;
+  return klaunch_chain(c->fp_mode == CGX_FP_FMA ? 1 : 0, c->order, c->d_descs, c->d_maps, c->d_tiles, c->ntiles,
+                       c->d_need, c->d_done, c->ncounters, c->d_ctl, c->d_status, (cudaStream_t)stream);
+}
+
+int cgx_chain_check(cgx_chain *c, void *stream) {
+  if (!c) return fail(CGX_EINVAL, "null chain");
+  if (!c->d_status) return CGX_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = 0;
+  cudaError_t e = cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "chain status read-back");
+  if (st) {
+    // the kernel resets its counters on exit; clear the status for reuse
+    e = cudaMemsetAsync(c->d_status, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return fail(CGX_EDEVICE, "chain: a bounded device wait gave up (status %d)", st);
+  }
+  return CGX_OK;
+}
+
+int cgx_chain_stats(const cgx_chain *c, int64_t *npairs, int64_t *ntiles, int64_t *dst_points,
+                    int64_t *bytes) {
+  if (!c) return fail(CGX_EINVAL, "null chain");
+  if (npairs) *npairs = c->pairs;
+  if (ntiles) *ntiles = c->ntiles;
+  if (dst_points) *dst_points = c->points;
+  if (bytes) *bytes = c->bytes;
+  return CGX_OK;
+}
+
+} // extern "C"
+
 // ============================================================== no-allocation form
 // cgx_transfer_pairs_noalloc runs a list of box-pairs through the persistent
 // kernel without allocating device memory.  The kernel's scratch -- the
@@ -1467,6 +1710,8 @@ extern "C" int cgx_noalloc_check(void *stream) {
 
 // ============================================================== internal API
 namespace cgx {
+
+thread_local int g_cta_cap[2] = {0, 0};
 
 int host_build(int op, int cent, const cgx_array *dst, const cgx_array *srcs, const double *times,
                int nsrc, const int *dstbox, const int *srcbox, const int *slab, double time,

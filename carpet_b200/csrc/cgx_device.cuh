@@ -350,6 +350,15 @@ template <class D> __host__ __device__ __forceinline__ int stream_variant(const 
   return d.tkind == T_ENO ? SV_COPY3E : SV_COPY3Q;
 }
 
+// Source loads of the streaming tiles: through the read-only path (__ldg)
+// in kernels whose sources no CTA of the same launch writes; cached in L2
+// only (__ldcg, coherent across SMs) in the chain kernel, whose later tiles
+// read what earlier tiles of the same launch wrote.
+template <bool CG> __device__ __forceinline__ double ld_src(const double *p) {
+  if (CG) return __ldcg(p);
+  return __ldg(p);
+}
+
 // floor(p / n) for 0 <= p < 2^31 (Granlund & Montgomery, "Division by
 // invariant integers using multiplication", 1994, theorem 4.2 with N = 31):
 // with l = ceil(log2 n), m = ceil(2^(31+l) / n) < 2^32 and s = l - 1,
@@ -372,12 +381,14 @@ template <int LANES, int NTL> __host__ __device__ constexpr int stream_group() {
   return (STILE / LANES) < (NTL == 1 ? 8 : 4) ? (STILE / LANES) : (NTL == 1 ? 8 : 4);
 }
 
-template <int FMA, int NTL, int TK, int LANES, class D>
+template <int FMA, int NTL, int TK, int LANES, class D, bool CG = false, int PTS = STILE, int GMAX = 8>
 __device__ __forceinline__ void copy_tile(const D &d, int tile, int lid) {
   // ENO time interpolation holds more per point: smaller groups
-  constexpr int PER = STILE / LANES, G = stream_group<LANES, NTL>() / (TK == T_ENO ? 2 : 1);
+  constexpr int PER = PTS / LANES;
+  constexpr int G0 = PER < (NTL == 1 ? GMAX : 4) ? PER : (NTL == 1 ? GMAX : 4);
+  constexpr int G = G0 / (TK == T_ENO ? 2 : 1);
   const unsigned npts = (unsigned)d.n[0] * d.n[1] * d.n[2];
-  const unsigned p0 = (unsigned)tile * STILE + lid;
+  const unsigned p0 = (unsigned)tile * PTS + lid;
   const double *src[NTL];
 #pragma unroll
   for (int t = 0; t < NTL; ++t) src[t] = d.src[t] + (d.soff[0] + d.soff[1] * d.ssy + d.soff[2] * d.ssz);
@@ -396,7 +407,7 @@ __device__ __forceinline__ void copy_tile(const D &d, int tile, int lid) {
         unflatten(d, p, i, j, k);
         const long long si = i + j * d.ssy + k * d.ssz;
 #pragma unroll
-        for (int t = 0; t < NTL; ++t) v[r][t] = __ldg(src[t] + si);
+        for (int t = 0; t < NTL; ++t) v[r][t] = ld_src<CG>(src[t] + si);
       }
     }
     // the destination index is recomputed rather than held across the loads
@@ -412,10 +423,11 @@ __device__ __forceinline__ void copy_tile(const D &d, int tile, int lid) {
   }
 }
 
-template <int LANES, class D> __device__ __forceinline__ void restrict_vc_tile(const D &d, int tile, int lid) {
-  constexpr int PER = STILE / LANES, G = stream_group<LANES, 1>();
+template <int LANES, class D, bool CG = false, int PTS = STILE, int GMAX = 8>
+__device__ __forceinline__ void restrict_vc_tile(const D &d, int tile, int lid) {
+  constexpr int PER = PTS / LANES, G = PER < GMAX ? PER : GMAX;
   const unsigned npts = (unsigned)d.n[0] * d.n[1] * d.n[2];
-  const unsigned p0 = (unsigned)tile * STILE + lid;
+  const unsigned p0 = (unsigned)tile * PTS + lid;
   const double *s = d.src[0] + (d.soff[0] + d.soff[1] * d.ssy + d.soff[2] * d.ssz);
   double *dst = d.dst + (d.doff[0] + d.doff[1] * d.dsy + d.doff[2] * d.dsz);
 #pragma unroll
@@ -427,7 +439,7 @@ template <int LANES, class D> __device__ __forceinline__ void restrict_vc_tile(c
       if (p < npts) {
         int i, j, k;
         unflatten(d, p, i, j, k);
-        v[r] = __ldg(s + 2 * (i + j * d.ssy + k * d.ssz));
+        v[r] = ld_src<CG>(s + 2 * (i + j * d.ssy + k * d.ssz));
       }
     }
 #pragma unroll

@@ -97,6 +97,27 @@ inline int segment_of(const Desc &d) {
   return v >= 0 ? v : SEG_STENCIL;
 }
 
+// One entry of a chain's tile list (cgx_chain.cuh): descriptor, tile
+// within it, the completion counter it increments, the counter it waits on
+// (-1: none).
+struct ChainTile {
+  int desc, tile, own, dep;
+};
+// control words of a chain launch: claim counter, exit counter, abort word
+constexpr int CHAIN_CTL_WORDS = 4;
+// the chain kernel of a floating-point mode and vertex-centred order
+// (cgx_kern_chain.cu)
+int klaunch_chain(int fp, int order, const Desc *d, const CUtensorMap *maps, const ChainTile *tiles,
+                  long long ntiles, const unsigned *need, unsigned *done, int ncounters,
+                  unsigned long long *ctl, int *status, cudaStream_t s);
+
+// CTAs per SM the persistent kernels of the launch in progress on this host
+// thread may use (0: as many as fit), [0] the TMA prolongation kernels, [1]
+// the streaming kernels; set by launch_map from the batch
+// (cgx_batch_set_max_ctas), read by the launchers.  A cap below the
+// occupancy limit leaves room on every SM for another stream's kernel.
+extern thread_local int g_cta_cap[2];
+
 int current_fp_mode();
 int set_error(int code, const char *fmt, ...);
 int cuda_error(cudaError_t e, const char *what);

@@ -40,12 +40,13 @@ cudaError_t launch_chained(void (*kernel)(P...), int grid, int block, size_t sme
 }
 
 template <class K>
-int persistent_grid(K kernel, size_t smem, long long ntiles, int *grid, int threads = NTHREADS) {
+int persistent_grid(K kernel, size_t smem, long long ntiles, int *grid, int threads = NTHREADS, int cap = 0) {
   int dev = 0, nsm = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
   if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+  if (cap > 0 && cap < per_sm) per_sm = cap;
   *grid = (int)std::min<long long>((long long)nsm * per_sm, ntiles);
   return CGX_OK;
 }
@@ -110,6 +111,7 @@ int launch_tma_v(int variant, const Desc *d_descs, const CUtensorMap *d_maps, co
           cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
+  if (g_cta_cap[0] > 0 && g_cta_cap[0] < per_sm) per_sm = g_cta_cap[0];
   const int grid = (int)std::min<long long>((long long)nsm * per_sm, ntiles);
   cudaError_t e = launch_chained(k_tma_map<FMA, F, NTL, TK, CFG>, grid, NT, smem, s, d_descs, d_maps, d_tmap,
                                  ntiles, d_counter, d_status, variant);
@@ -136,7 +138,7 @@ template <int FMA, int V>
 int launch_stream_v(const Desc *d_descs, const int2 *d_tmap, long long ntiles,
                     unsigned long long *d_counter, int *d_status, cudaStream_t s) {
   int grid = 0;
-  persistent_grid(k_stream_map<FMA, V>, 0, ntiles, &grid, STREAM_THREADS);
+  persistent_grid(k_stream_map<FMA, V>, 0, ntiles, &grid, STREAM_THREADS, g_cta_cap[1]);
   cudaError_t e = launch_chained(k_stream_map<FMA, V>, grid, STREAM_THREADS, 0, s, d_descs, d_tmap, ntiles,
                                  d_counter, d_status);
   return e == cudaSuccess ? CGX_OK : cuda_error(e, "k_stream_map launch");

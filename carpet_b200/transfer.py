@@ -131,7 +131,7 @@ class Batch:
         self.h = h
 
     def __del__(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and lib is not None:
             lib.cgx_batch_destroy(self.h)
             self.h = None
 
@@ -170,6 +170,16 @@ class Batch:
         vp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
         check(lib.cgx_batch_add_many(self.h, op, cent, arr, len(pairs), vp(di), vp(si), nsrc, ts, vp(db),
                                      vp(sb), float(time), int(order_space), int(order_time)))
+
+    def set_max_ctas(self, tma_per_sm: int = 0, stream_per_sm: int = 0):
+        """CTAs per SM of the batch's TMA prolongation and streaming kernels
+        (0: as many as fit); room for another stream's kernel on every SM"""
+        check(lib.cgx_batch_set_max_ctas(self.h, int(tma_per_sm), int(stream_per_sm)))
+
+    def set_group(self, group: int):
+        """pairs added from now on belong to dependency group ``group``
+        (cgx_batch_set_group; used by Chain)"""
+        check(lib.cgx_batch_set_group(self.h, int(group)))
 
     def add_raw(self, op, cent, dst: cgx_array, srcs_arr, ts, nsrc, dstbox, srcbox, time,
                 order_space, order_time):
@@ -214,6 +224,43 @@ class Batch:
         check(lib.cgx_batch_check(self.h, _stream(stream)))
 
 
+class Chain:
+    """A sequence of batches run as one persistent launch (cgx_chain_*):
+    each dependency group (Batch.set_group) sees the batches in order, the
+    groups' tiles share the GPU.  The batches must outlive the chain."""
+
+    def __init__(self, batches=()):
+        h = C.c_void_p()
+        check(lib.cgx_chain_create(C.byref(h)))
+        self.h = h
+        self.batches = []
+        for b in batches:
+            self.add(b)
+
+    def __del__(self):
+        if getattr(self, "h", None) and lib is not None:
+            lib.cgx_chain_destroy(self.h)
+            self.h = None
+
+    def add(self, b: Batch):
+        check(lib.cgx_chain_add(self.h, b.h))
+        self.batches.append(b)
+
+    def upload(self, stream=None):
+        check(lib.cgx_chain_upload(self.h, _stream(stream)))
+
+    def launch(self, stream=None):
+        check(lib.cgx_chain_launch(self.h, _stream(stream)))
+
+    def check(self, stream=None):
+        check(lib.cgx_chain_check(self.h, _stream(stream)))
+
+    def stats(self):
+        v = [C.c_int64() for _ in range(4)]
+        check(lib.cgx_chain_stats(self.h, *[C.byref(x) for x in v]))
+        return dict(pairs=v[0].value, tiles=v[1].value, points=v[2].value, bytes=v[3].value)
+
+
 class Graph:
     """CUDA graph of the calls made inside ``with g.capture(stream):``."""
 
@@ -241,6 +288,6 @@ class Graph:
         check(lib.cgx_graph_launch(self.h, _stream(stream)))
 
     def __del__(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and lib is not None:
             lib.cgx_graph_destroy(self.h)
             self.h = None

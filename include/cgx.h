@@ -176,6 +176,14 @@ int cgx_batch_autotune(cgx_batch *b, int reps, void *stream, int *chosen);
  * variant, or of all with variant = -1 (e.g. a saved autotune result);
  * takes effect at the next cgx_batch_upload */
 int cgx_batch_set_config(cgx_batch *b, int variant, int config);
+/* CTAs per SM that the batch's persistent kernels may use: tma_per_sm for
+ * the TMA prolongation kernels, stream_per_sm for the streaming (copy,
+ * restriction) kernels; 0 = as many as fit (the default).  Below the
+ * occupancy limit, a batch leaves room on every SM for a kernel on another
+ * stream (the grid functions of another group), so that a compute-bound
+ * prolongation and a memory-bound sync can run on the same SMs at once.
+ * Takes effect at the next launch.  No counterpart in the reference. */
+int cgx_batch_set_max_ctas(cgx_batch *b, int tma_per_sm, int stream_per_sm);
 /* plain per-box launches of the same descriptors (one kernel per pair) */
 int cgx_batch_launch_per_box(cgx_batch *b, void *stream);
 /* ---- host schedules: the send/recv region lists of dh (CarpetLib/src/
@@ -254,6 +262,40 @@ int cgx_server_replay(cgx_server *s, const int *op_ids, const double *arrival_s,
 int cgx_server_drain(cgx_server *s); /* wait until every submitted request is done */
 int cgx_server_stats(cgx_server *s, cgx_server_report *rep);
 int cgx_server_latencies(cgx_server *s, double *out_ms, int64_t n);
+
+/*
+ * Chain form: a sequence of batches as ONE persistent launch.  NO
+ * COUNTERPART IN THE REFERENCE, which makes the same transfers one call at a
+ * time (the phases of a Berger-Oliger step: Carpet/src/Evolve.cc:44-121).
+ *
+ * cgx_batch_set_group(b, g) tags the pairs added to b afterwards with the
+ * dependency group g (default 0): pairs of different groups must touch
+ * disjoint arrays throughout the chain -- one grid function per group, say.
+ * cgx_chain_add appends batches in call order; cgx_chain_upload builds one
+ * tile list over all of them.  In the launch, a tile of batch j and group g
+ * starts once every tile of the latest earlier batch with pairs of group g
+ * has completed, so each group sees the batches in order while the groups'
+ * tiles of different batches share the GPU.  The result equals running the
+ * batches one after another (bit for bit).  Accepted pairs: vertex-centred
+ * Lagrange prolongation of one order (1, 3 or 5) with one timelevel or
+ * quadratic time interpolation over three, on arrays TMA can stage (16-byte
+ * aligned base, even row and plane pitch); one-timelevel copies; injection.
+ * Anything else returns CGX_EUNSUPPORTED at upload.  The floating-point mode
+ * is the one current at upload.  The batches must stay alive and unchanged
+ * while the chain is used; cgx_chain_upload reads them, the launch does not.
+ * Every device wait is bounded; cgx_chain_check reports CGX_EDEVICE if one
+ * gave up.  Capturable in a CUDA graph.
+ */
+typedef struct cgx_chain cgx_chain;
+int cgx_batch_set_group(cgx_batch *b, int group);
+int cgx_chain_create(cgx_chain **out);
+int cgx_chain_destroy(cgx_chain *c);
+int cgx_chain_add(cgx_chain *c, cgx_batch *b);
+int cgx_chain_upload(cgx_chain *c, void *stream);
+int cgx_chain_launch(cgx_chain *c, void *stream);
+int cgx_chain_check(cgx_chain *c, void *stream);
+int cgx_chain_stats(const cgx_chain *c, int64_t *npairs, int64_t *ntiles, int64_t *dst_points,
+                    int64_t *bytes);
 
 /*
  * No-allocation form.  NO COUNTERPART IN THE REFERENCE: CarpetLib has no
