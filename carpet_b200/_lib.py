@@ -79,6 +79,8 @@ lib.cgx_find_source_timelevel.argtypes = [_P(C.c_double), C.c_int, C.c_double, C
 lib.cgx_stream_sync.argtypes = [C.c_void_p]
 lib.cgx_batch_set_group.argtypes = [C.c_void_p, C.c_int]
 lib.cgx_batch_set_max_ctas.argtypes = [C.c_void_p, C.c_int, C.c_int]
+lib.cgx_debug_skip_tma_plane.argtypes = [C.c_int]
+lib.cgx_chain_debug_hold.argtypes = [C.c_void_p, C.c_int]
 lib.cgx_chain_create.argtypes = [_P(C.c_void_p)]
 lib.cgx_chain_destroy.argtypes = [C.c_void_p]
 lib.cgx_chain_add.argtypes = [C.c_void_p, C.c_void_p]

@@ -706,6 +706,10 @@ const TmaLaunch kTmaLaunch[2][2][TMA_NCFG] = {{CGX_TMA_ROW(0, 0), CGX_TMA_ROW(0,
 int launch_map_capped(int fp, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
                       const long long seg[NSEG + 1], const int *cfg, unsigned long long *counter, int *status,
                       cudaStream_t s);
+// failure injection for the tests of the bounded device waits
+// (cgx_debug_skip_tma_plane)
+bool g_debug_skip_tma = false;
+
 // with the batch's CTA caps in force for these launches only
 int launch_map(int fp, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
                const long long seg[NSEG + 1], const int *cfg, unsigned long long *counter, int *status,
@@ -729,7 +733,7 @@ int launch_map_capped(int fp, const Desc *d, const CUtensorMap *maps, const int2
     if (i < TV_COUNT) {
       const int k = cfg ? cfg[i] : 0;
       if (k < 0 || k >= TMA_NCFG) return fail(CGX_EINVAL, "bad tile configuration %d", k);
-      rc = kTmaLaunch[f][i / 4 >= 5][k](i, d, maps, tm, n, c, status, s);
+      rc = kTmaLaunch[f][i / 4 >= 5][k](i | (g_debug_skip_tma ? 1 << 30 : 0), d, maps, tm, n, c, status, s);
     } else if (i == SEG_STENCIL) {
       rc = f ? klaunch_map_f1(d, tm, n, c, status, s) : klaunch_map_f0(d, tm, n, c, status, s);
     } else {
@@ -943,6 +947,11 @@ int cgx_batch_clear(cgx_batch *b) {
   b->cur_group = 0;
   b->tmp_elems = 0;
   b->nstage1 = 0;
+  return CGX_OK;
+}
+
+int cgx_debug_skip_tma_plane(int enable) {
+  g_debug_skip_tma = enable != 0;
   return CGX_OK;
 }
 
@@ -1384,6 +1393,7 @@ int cgx_stream_sync(void *stream) {
 // batches' host-side pairs.
 struct cgx_chain {
   std::vector<cgx_batch *> batches;
+  bool debug_hold = false; // cgx_chain_debug_hold
   int order = -1; // vertex-centred prolongation order of every prolongation pair
   int fp_mode = CGX_FP_EXACT;
   Desc *d_descs = nullptr;
@@ -1429,6 +1439,12 @@ int cgx_chain_destroy(cgx_chain *c) {
   if (!c) return CGX_OK;
   chain_free(c);
   delete c;
+  return CGX_OK;
+}
+
+int cgx_chain_debug_hold(cgx_chain *c, int hold) {
+  if (!c) return fail(CGX_EINVAL, "null chain");
+  c->debug_hold = hold != 0;
   return CGX_OK;
 }
 
@@ -1505,6 +1521,8 @@ int cgx_chain_upload(cgx_chain *c, void *stream) {
   }
   if (hd.size() >= (size_t)INT_MAX || ht.size() >= (size_t)INT_MAX)
     return fail(CGX_EINVAL, "chain: too many pairs or tiles");
+  if (c->debug_hold) // failure injection: no dependency is ever satisfied
+    for (unsigned &n : need) n += 1;
   chain_free(c);
   const size_t nd = std::max<size_t>(hd.size(), 1), nt = std::max<size_t>(ht.size(), 1),
                nc = std::max<size_t>(need.size(), 1);

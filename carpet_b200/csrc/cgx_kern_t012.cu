@@ -5,7 +5,7 @@
 namespace cgx {
 int klaunch_tma_f0_p1_c2(int variant, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
                          long long ntiles, unsigned long long *counter, int *status, cudaStream_t s) {
-  switch (variant / 4) {
+  switch ((variant & ~(1 << 30)) / 4) { // bit 30: failure injection
   case 5: return kern::launch_tma_family<0, CC<2>, 2>(variant, d, maps, tmap, ntiles, counter, status, s);
   case 6: return kern::launch_tma_family<0, CC<3>, 2>(variant, d, maps, tmap, ntiles, counter, status, s);
   case 7: return kern::launch_tma_family<0, CC<4>, 2>(variant, d, maps, tmap, ntiles, counter, status, s);

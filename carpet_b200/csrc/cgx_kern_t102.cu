@@ -5,7 +5,7 @@
 namespace cgx {
 int klaunch_tma_f1_p0_c2(int variant, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
                          long long ntiles, unsigned long long *counter, int *status, cudaStream_t s) {
-  switch (variant / 4) {
+  switch ((variant & ~(1 << 30)) / 4) { // bit 30: failure injection
   case 0: return kern::launch_tma_family<1, VC<1>, 2>(variant, d, maps, tmap, ntiles, counter, status, s);
   case 1: return kern::launch_tma_family<1, VC<3>, 2>(variant, d, maps, tmap, ntiles, counter, status, s);
   case 2: return kern::launch_tma_family<1, VC<5>, 2>(variant, d, maps, tmap, ntiles, counter, status, s);

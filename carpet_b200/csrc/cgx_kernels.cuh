@@ -354,6 +354,9 @@ __global__ void __launch_bounds__(TMA_CFGS[CFG].nt, TMA_CFGS[CFG].mb)
   __shared__ __align__(16) Desc s_d;
   __shared__ __align__(8) uint64_t s_bars[TMA_NB_MAX];
   __shared__ int s_abort;
+  // bit 30 of variant: failure injection (cgx_debug_skip_tma_plane)
+  const int skip = (variant >> 30) & 1 ? 0 : -1;
+  variant &= ~(1 << 30);
   pdl_wait();
   if (threadIdx.x == 0) {
     for (int i = 0; i < TMA_NB_MAX; ++i) mbar_init(&s_bars[i], 1);
@@ -364,7 +367,7 @@ __global__ void __launch_bounds__(TMA_CFGS[CFG].nt, TMA_CFGS[CFG].mb)
     s_m = t < ntiles ? tmap[t] : make_int2(0, 0);
   }
   __syncthreads();
-  TmaRing ring{s_bars, &s_abort, 0u};
+  TmaRing ring{s_bars, &s_abort, 0u, skip};
   for (;;) {
     if (s_t >= ntiles) {
       if (threadIdx.x == 0) claims_done(counter);

@@ -123,6 +123,10 @@ struct TmaRing {
   uint64_t *bars; // pd + 2 mbarriers, arrival count 1
   int *abort;     // shared flag, set when a wait gave up
   unsigned g;     // planes staged by this CTA before the current tile
+  // failure injection for the tests of the bounded waits
+  // (cgx_debug_skip_tma_plane): the plane of this CTA's first tile that is
+  // never staged, so that the wait for it runs out; -1 in normal use
+  int skip = -1;
 };
 
 // One prolongation tile.  Returns false when a wait gave up (the CTA then
@@ -161,8 +165,10 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
   double *xrows = sm + S::coarse;
 
   int issued = 0; // planes staged so far (elected thread)
+  const int skip = g0 == 0 ? ring.skip : -1;
   auto issue = [&](int p) { // elected thread: stage plane p
     issued = p + 1;
+    if (p == skip) return; // failure injection: this plane never lands
     const unsigned g = g0 + (unsigned)p;
     const int slot = (int)(g % NB);
     mbar_expect_tx(&ring.bars[slot], (unsigned)(NTL * BX * BY * 8));
@@ -329,6 +335,7 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
     if (tid == 0) {
       if (status) atomicCAS(status, 0, CGX_EDEVICE);
       for (int i = 0; i < issued; ++i) {
+        if (i == skip) continue;
         const unsigned g = g0 + (unsigned)i;
         mbar_wait_bounded(&ring.bars[g % NB], (g / NB) & 1);
       }

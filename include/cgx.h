@@ -298,6 +298,24 @@ int cgx_chain_stats(const cgx_chain *c, int64_t *npairs, int64_t *ntiles, int64_
                     int64_t *bytes);
 
 /*
+ * Failure injection, for the tests of the bounded device waits.  NO
+ * COUNTERPART IN THE REFERENCE.  Every wait of the kernels on a device event
+ * (a TMA copy landing on its mbarrier, a chain tile's dependency counter)
+ * gives up after about 2^31 clock cycles (a second), records CGX_EDEVICE in
+ * the launch's status word and lets the launch drain, so that the context
+ * stays usable; the batch / chain check then reports CGX_EDEVICE.
+ *   cgx_debug_skip_tma_plane(1): the TMA prolongation kernels launched from
+ *     now on never stage the first plane of each CTA's first tile, so that
+ *     the wait for it runs out (0 restores normal operation);
+ *   cgx_chain_debug_hold(c, 1): the next cgx_chain_upload of c requires one
+ *     more completed tile of every counter than exists, so that every
+ *     dependency wait runs out (0 and a new upload restore it).
+ * Off by default; process-wide (the first) or per chain (the second).
+ */
+int cgx_debug_skip_tma_plane(int enable);
+int cgx_chain_debug_hold(cgx_chain *c, int hold);
+
+/*
  * No-allocation form.  NO COUNTERPART IN THE REFERENCE: CarpetLib has no
  * device path at all; this entry point exists for callers of this library
  * that must not allocate device memory -- code that runs while a CUDA graph
