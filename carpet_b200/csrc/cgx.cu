@@ -1153,50 +1153,13 @@ static int ensure_side_streams(cgx_batch *b) {
 }
 
 static int launch_segments(cgx_batch *b, cudaStream_t s) {
-  constexpr int TSEG = SEG_STREAM + SV_TIME;
-  static_assert(TSEG == NSEG - 1, "the time combination is the last segment");
-  int idx[NSEG];
-  const int n = concurrent_segments(b, idx);
-  if (n <= 1)
-    return launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, b->seg, b->tma_cfg, b->d_counter,
-                      b->d_status, s, b->max_ctas);
-  const size_t nside = (size_t)n - 1;
-  if (b->side.size() < nside || b->ev.size() < nside + 1)
+  int need = 0;
+  const int rc = launch_map_concurrent(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, b->seg, b->tma_cfg,
+                                       b->d_counter, b->d_status, s, b->side.data(), b->ev.data(),
+                                       (int)std::min(b->side.size(), b->ev.size() ? b->ev.size() - 1 : 0),
+                                       &need, b->max_ctas);
+  if (rc == CGX_EINVAL && need > 0)
     return fail(CGX_EINVAL, "batch launch: the batch was not uploaded on this device");
-  // a segment array in which only segment i is non-empty
-  auto only = [&](int i, long long *sg) {
-    for (int k = 0; k <= NSEG; ++k) sg[k] = k <= i ? b->seg[i] : b->seg[i + 1];
-  };
-  // fork: every side stream that has waited on ev[0] is joined below, also
-  // when a later fork step or a launch fails (a capture stays joined)
-  size_t forked = 0;
-  cudaError_t e = cudaEventRecord(b->ev[0], s);
-  while (e == cudaSuccess && forked < nside) {
-    e = cudaStreamWaitEvent(b->side[forked], b->ev[0], 0);
-    if (e == cudaSuccess) ++forked;
-  }
-  int rc = e != cudaSuccess ? cuda_fail(e, "fork of the segment streams") : CGX_OK;
-  for (int j = 0; j < n && rc == CGX_OK; ++j) {
-    long long sg[NSEG + 1];
-    only(idx[j], sg);
-    rc = launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, sg, b->tma_cfg, b->d_counter, b->d_status,
-                    j == 0 ? s : b->side[j - 1], b->max_ctas);
-  }
-  // join every forked side stream, also after a failure
-  cudaError_t je = cudaSuccess;
-  for (size_t k = 0; k < forked; ++k) {
-    cudaError_t r = cudaEventRecord(b->ev[1 + k], b->side[k]);
-    if (r == cudaSuccess) r = cudaStreamWaitEvent(s, b->ev[1 + k], 0);
-    if (r != cudaSuccess && je == cudaSuccess) je = r;
-  }
-  if (rc) return rc;
-  if (je != cudaSuccess) return cuda_fail(je, "join of the segment streams");
-  if (b->seg[TSEG + 1] > b->seg[TSEG]) {
-    long long sg[NSEG + 1];
-    only(TSEG, sg);
-    rc = launch_map(b->fp_mode, b->d_descs, b->d_maps, b->d_tmap, sg, b->tma_cfg, b->d_counter, b->d_status, s,
-                    b->max_ctas);
-  }
   return rc;
 }
 
@@ -1729,6 +1692,57 @@ extern "C" int cgx_noalloc_check(void *stream) {
 // ============================================================== internal API
 namespace cgx {
 
+int launch_map_concurrent(int fp, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
+                          const long long seg[NSEG + 1], const int *cfg, unsigned long long *counter,
+                          int *status, cudaStream_t s, const cudaStream_t *side, const cudaEvent_t *ev,
+                          int nside_have, int *need, const int *caps) {
+  constexpr int TSEG = SEG_STREAM + SV_TIME;
+  static_assert(TSEG == NSEG - 1, "the time combination is the last segment");
+  int idx[NSEG], n = 0;
+  for (int i = 0; i < TSEG; ++i)
+    if (seg[i + 1] > seg[i]) idx[n++] = i;
+  *need = 0;
+  if (n <= 1) return launch_map(fp, d, maps, tmap, seg, cfg, counter, status, s, caps);
+  const int nside = n - 1;
+  if (nside_have < nside) {
+    *need = nside;
+    return fail(CGX_EINVAL, "concurrent launch: %d side streams needed, %d given", nside, nside_have);
+  }
+  // a segment array in which only segment i is non-empty
+  auto only = [&](int i, long long *sg) {
+    for (int k = 0; k <= NSEG; ++k) sg[k] = k <= i ? seg[i] : seg[i + 1];
+  };
+  // fork: every side stream that has waited on ev[0] is joined below, also
+  // when a later fork step or a launch fails (a capture stays joined)
+  int forked = 0;
+  cudaError_t e = cudaEventRecord(ev[0], s);
+  while (e == cudaSuccess && forked < nside) {
+    e = cudaStreamWaitEvent(side[forked], ev[0], 0);
+    if (e == cudaSuccess) ++forked;
+  }
+  int rc = e != cudaSuccess ? cuda_fail(e, "fork of the segment streams") : CGX_OK;
+  for (int j = 0; j < n && rc == CGX_OK; ++j) {
+    long long sg[NSEG + 1];
+    only(idx[j], sg);
+    rc = launch_map(fp, d, maps, tmap, sg, cfg, counter, status, j == 0 ? s : side[j - 1], caps);
+  }
+  // join every forked side stream, also after a failure
+  cudaError_t je = cudaSuccess;
+  for (int k = 0; k < forked; ++k) {
+    cudaError_t r = cudaEventRecord(ev[1 + k], side[k]);
+    if (r == cudaSuccess) r = cudaStreamWaitEvent(s, ev[1 + k], 0);
+    if (r != cudaSuccess && je == cudaSuccess) je = r;
+  }
+  if (rc) return rc;
+  if (je != cudaSuccess) return cuda_fail(je, "join of the segment streams");
+  if (seg[TSEG + 1] > seg[TSEG]) {
+    long long sg[NSEG + 1];
+    only(TSEG, sg);
+    rc = launch_map(fp, d, maps, tmap, sg, cfg, counter, status, s, caps);
+  }
+  return rc;
+}
+
 thread_local int g_cta_cap[2] = {0, 0};
 
 int host_build(int op, int cent, const cgx_array *dst, const cgx_array *srcs, const double *times,
@@ -1747,7 +1761,7 @@ int host_build(int op, int cent, const cgx_array *dst, const cgx_array *srcs, co
 }
 
 int batch_pairs(const cgx_batch *b, const Desc **descs, const int **ntiles, const long long **points,
-                int *n) {
+                const long long **bytes, int *n) {
   if (!b) return fail(CGX_EINVAL, "null batch");
   for (size_t i = 0; i < b->high.size(); ++i)
     if (b->high[i]) return fail(CGX_EUNSUPPORTED, "vertex-centred orders 7-11 cannot be served");
@@ -1756,6 +1770,7 @@ int batch_pairs(const cgx_batch *b, const Desc **descs, const int **ntiles, cons
   *descs = b->descs.data();
   *ntiles = b->ntiles.data();
   *points = b->points.data();
+  *bytes = b->bytes.data();
   *n = (int)b->descs.size();
   return CGX_OK;
 }

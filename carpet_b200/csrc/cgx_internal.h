@@ -26,7 +26,7 @@ int host_build(int op, int cent, const cgx_array *dst, const cgx_array *srcs, co
 
 // The host-side descriptors of a batch (cgx.cu).
 int batch_pairs(const cgx_batch *b, const Desc **descs, const int **ntiles, const long long **points,
-                int *n);
+                const long long **bytes, int *n);
 
 // A tile map is laid out in segments, one persistent kernel each: segment v
 // < TV_COUNT holds the prolongation tiles of TMA variant v, segment
@@ -44,6 +44,17 @@ constexpr int NSEG = SEG_STREAM + SV_COUNT;
 int launch_tile_map(const Desc *d_descs, const CUtensorMap *d_maps, const int2 *d_tmap,
                     const long long seg[NSEG + 1], unsigned long long *d_counter, int *d_status, int fp,
                     cudaStream_t s);
+
+// The segments of a tile map launched concurrently (cgx.cu): every
+// non-empty segment but the time combination on a stream of its own
+// (side[0 .. nside-1], forked from s with ev[0] and joined back with
+// ev[1 + k]), then the time segment on s; nside + 1 events.  Returns the
+// number of side streams needed in *need when they do not suffice.
+int launch_map_concurrent(int fp, const Desc *d, const CUtensorMap *maps, const int2 *tmap,
+                          const long long seg[NSEG + 1], const int *cfg, unsigned long long *counter,
+                          int *status, cudaStream_t s, const cudaStream_t *side, const cudaEvent_t *ev,
+                          int nside, int *need, const int *caps = nullptr);
+constexpr int CONCURRENT_SIDE_MAX = NSEG;
 
 // The tensor maps of a prolongation descriptor's source timelevels (cgx.cu):
 // true when the arrays can be staged by TMA (then maps[0 .. ntl-1] are

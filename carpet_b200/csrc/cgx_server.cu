@@ -18,7 +18,14 @@
 // request at a time, one kernel launch per box-pair.
 //
 // Hierarchies are admitted against an HBM budget (cgx_server_admit /
-// cgx_server_release account the device memory their grid functions use).
+// cgx_server_release account the device memory their grid functions use),
+// also while the worker runs: operations of a newly admitted hierarchy can be
+// defined at any time, and its requests join the stream from then on.
+//
+// A slot launches the concatenated requests' segments (prolongation kinds,
+// copies, restrictions) concurrently: each non-empty segment but the last on
+// a side stream of the slot, forked from and joined back into the slot's
+// stream, so that a mixed launch's kernels share the GPU.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -45,7 +52,7 @@ struct OpTemplate {
   std::vector<Desc> descs;
   std::vector<CUtensorMap> maps; // 3 per descriptor (prolongation staged by TMA)
   std::vector<int> ntiles;
-  long long tiles = 0, points = 0;
+  long long tiles = 0, points = 0, bytes = 0;
 };
 
 struct Request {
@@ -56,6 +63,9 @@ struct Request {
 struct Slot {
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
+  // the concurrent segment launch: side streams, fork and join events
+  cudaStream_t side[CONCURRENT_SIDE_MAX] = {};
+  cudaEvent_t ev[CONCURRENT_SIDE_MAX + 1] = {};
   Desc *d_descs = nullptr, *h_descs = nullptr;
   int2 *d_tmap = nullptr, *h_tmap = nullptr;
   CUtensorMap *d_maps = nullptr, *h_maps = nullptr;
@@ -64,6 +74,10 @@ struct Slot {
   size_t desc_cap = 0, tile_cap = 0;
   bool busy = false;
   std::vector<int> reqs;
+  // set by the host function enqueued behind the slot's launch (a CUDA
+  // driver thread), read by the worker under the server's mutex
+  bool landed = false;
+  struct cgx_server *owner = nullptr;
 };
 
 } // namespace
@@ -72,7 +86,10 @@ struct cgx_server {
   int mode = CGX_SERVE_BATCHED;
   int fp = CGX_FP_EXACT;
   long long budget = 0, used = 0;
-  std::vector<OpTemplate> ops;
+  // operations: appended under mu (also while the worker runs); a deque
+  // keeps the address of every element, which the worker uses after
+  // releasing the lock
+  std::deque<OpTemplate> ops;
   std::vector<Request> reqs; // reserved at creation: never reallocated
   size_t max_requests = 0;
   std::vector<char> hier_busy;
@@ -107,6 +124,10 @@ int slot_init(Slot &s, size_t desc_cap, size_t tile_cap) {
   if (e == cudaSuccess) e = cudaMemset(s.d_counter, 0, 2 * NSEG * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMalloc(&s.d_status, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(s.d_status, 0, sizeof(int));
+  for (int k = 0; k < CONCURRENT_SIDE_MAX && e == cudaSuccess; ++k)
+    e = cudaStreamCreateWithFlags(&s.side[k], cudaStreamNonBlocking);
+  for (int k = 0; k <= CONCURRENT_SIDE_MAX && e == cudaSuccess; ++k)
+    e = cudaEventCreateWithFlags(&s.ev[k], cudaEventDisableTiming);
   if (e != cudaSuccess) return cuda_error(e, "server slot allocation");
   s.desc_cap = desc_cap;
   s.tile_cap = tile_cap;
@@ -124,9 +145,16 @@ void slot_free(Slot &s) {
   cudaFree(s.d_counter);
   cudaFree(s.d_status);
   if (s.done) cudaEventDestroy(s.done);
+  for (cudaStream_t x : s.side)
+    if (x) cudaStreamDestroy(x);
+  for (cudaEvent_t x : s.ev)
+    if (x) cudaEventDestroy(x);
   if (s.stream) cudaStreamDestroy(s.stream);
   s = Slot();
 }
+
+// Host function behind a slot's launch: wakes the worker (no CUDA calls).
+void CUDART_CB slot_landed(void *arg);
 
 // Retire a slot whose kernel has finished.
 void retire(cgx_server *sv, Slot &s) {
@@ -139,6 +167,7 @@ void retire(cgx_server *sv, Slot &s) {
   sv->completed += (long long)s.reqs.size();
   s.reqs.clear();
   s.busy = false;
+  s.landed = false;
   sv->cv.notify_all();
 }
 
@@ -146,6 +175,7 @@ void retire(cgx_server *sv, Slot &s) {
 // (in arrival order) that fits the slot, and launch them as one kernel.
 bool launch_batch(cgx_server *sv, Slot &s) {
   std::vector<int> take;
+  std::vector<const OpTemplate *> tops; // the taken requests' operations
   size_t ndesc = 0, ntiles = 0;
   {
     std::lock_guard<std::mutex> g(sv->mu);
@@ -170,6 +200,7 @@ bool launch_batch(cgx_server *sv, Slot &s) {
         continue;
       }
       take.push_back(*it);
+      tops.push_back(&op);
       ndesc += op.descs.size();
       ntiles += op.tiles;
       sv->hier_busy[op.hier] = 1;
@@ -182,32 +213,42 @@ bool launch_batch(cgx_server *sv, Slot &s) {
   // variant's), one persistent kernel per segment
   size_t di = 0, ti = 0;
   const double t = sv->now();
-  for (int r : take) {
-    const OpTemplate &op = sv->ops[sv->reqs[r].op];
+  for (size_t q = 0; q < take.size(); ++q) {
+    const OpTemplate &op = *tops[q];
     for (size_t k = 0; k < op.descs.size(); ++k) {
       for (int j = 0; j < 3; ++j) s.h_maps[3 * di + j] = op.maps[3 * k + j];
       s.h_descs[di++] = op.descs[k];
     }
-    sv->reqs[r].t_launch = t;
+    sv->reqs[take[q]].t_launch = t;
   }
   long long seg[NSEG + 1];
   for (int g = 0; g < NSEG; ++g) {
     seg[g] = (long long)ti;
     size_t d0 = 0;
-    for (int r : take) {
-      const OpTemplate &op = sv->ops[sv->reqs[r].op];
-      for (size_t k = 0; k < op.descs.size(); ++k, ++d0)
-        if (segment_of(op.descs[k]) == g)
-          for (int j = 0; j < op.ntiles[k]; ++j) s.h_tmap[ti++] = make_int2((int)d0, j);
-    }
+    for (const OpTemplate *op : tops)
+      for (size_t k = 0; k < op->descs.size(); ++k, ++d0)
+        if (segment_of(op->descs[k]) == g)
+          for (int j = 0; j < op->ntiles[k]; ++j) s.h_tmap[ti++] = make_int2((int)d0, j);
   }
   seg[NSEG] = (long long)ti;
-  cudaMemcpyAsync(s.d_descs, s.h_descs, di * sizeof(Desc), cudaMemcpyHostToDevice, s.stream);
-  cudaMemcpyAsync(s.d_tmap, s.h_tmap, ti * sizeof(int2), cudaMemcpyHostToDevice, s.stream);
-  cudaMemcpyAsync(s.d_maps, s.h_maps, 3 * di * sizeof(CUtensorMap), cudaMemcpyHostToDevice, s.stream);
-  int rc = launch_tile_map(s.d_descs, s.d_maps, s.d_tmap, seg, s.d_counter, s.d_status, sv->fp, s.stream);
+  cudaError_t e = cudaMemcpyAsync(s.d_descs, s.h_descs, di * sizeof(Desc), cudaMemcpyHostToDevice, s.stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(s.d_tmap, s.h_tmap, ti * sizeof(int2), cudaMemcpyHostToDevice, s.stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(s.d_maps, s.h_maps, 3 * di * sizeof(CUtensorMap), cudaMemcpyHostToDevice, s.stream);
+  int rc = e == cudaSuccess ? CGX_OK : cuda_error(e, "server slot upload");
+  if (rc == CGX_OK && seg[NSEG] > 0) {
+    e = cudaMemsetAsync(s.d_counter, 0, NSEG * sizeof(unsigned long long), s.stream);
+    int need = 0;
+    rc = e == cudaSuccess ? launch_map_concurrent(sv->fp, s.d_descs, s.d_maps, s.d_tmap, seg, nullptr,
+                                                  s.d_counter, s.d_status, s.stream, s.side, s.ev,
+                                                  CONCURRENT_SIDE_MAX, &need)
+                          : cuda_error(e, "cudaMemsetAsync");
+  }
   if (rc) sv->error = rc;
-  cudaEventRecord(s.done, s.stream);
+  e = cudaEventRecord(s.done, s.stream);
+  if (e == cudaSuccess) e = cudaLaunchHostFunc(s.stream, slot_landed, &s);
+  if (e != cudaSuccess && !sv->error) sv->error = cuda_error(e, "slot completion");
   s.reqs = take;
   s.busy = true;
   sv->launches++;
@@ -218,19 +259,23 @@ bool launch_batch(cgx_server *sv, Slot &s) {
 // Plain mode: one request, one launch per box-pair, in arrival order.
 bool launch_plain(cgx_server *sv, Slot &s) {
   int r;
+  const OpTemplate *opp;
   {
     std::lock_guard<std::mutex> g(sv->mu);
     if (sv->pending.empty()) return false;
     r = sv->pending.front();
     sv->pending.pop_front();
+    opp = &sv->ops[sv->reqs[r].op];
   }
-  const OpTemplate &op = sv->ops[sv->reqs[r].op];
+  const OpTemplate &op = *opp;
   sv->reqs[r].t_launch = sv->now();
   for (size_t k = 0; k < op.descs.size(); ++k) {
     int rc = launch_one_pair(op.descs[k], op.ntiles[k], sv->fp, s.d_status, s.stream);
     if (rc) sv->error = rc;
   }
-  cudaEventRecord(s.done, s.stream);
+  cudaError_t e = cudaEventRecord(s.done, s.stream);
+  if (e == cudaSuccess) e = cudaLaunchHostFunc(s.stream, slot_landed, &s);
+  if (e != cudaSuccess && !sv->error) sv->error = cuda_error(e, "slot completion");
   s.reqs.assign(1, r);
   s.busy = true;
   sv->launches += (long long)op.descs.size();
@@ -264,7 +309,18 @@ void worker_loop(cgx_server *sv) {
       if (sv->pending.empty()) return;
     }
     if (any_busy) {
-      std::this_thread::yield(); // poll the in-flight slots
+      // sleep until a slot's launch lands (its host function notifies) or
+      // a request arrives that a free slot could take; the bound only
+      // guards against a missed notification
+      std::unique_lock<std::mutex> g(sv->mu);
+      sv->cv.wait_for(g, std::chrono::milliseconds(2), [&] {
+        bool landed = false, free_slot = false;
+        for (int i = 0; i < nslots; ++i) {
+          landed |= sv->slots[i].busy && sv->slots[i].landed;
+          free_slot |= !sv->slots[i].busy;
+        }
+        return landed || (free_slot && !sv->pending.empty()) || sv->stop.load();
+      });
     } else {
       std::unique_lock<std::mutex> g(sv->mu);
       sv->cv.wait_for(g, std::chrono::microseconds(200),
@@ -281,6 +337,16 @@ double percentile(std::vector<double> v, double p) {
   size_t hi = std::min(lo + 1, v.size() - 1);
   double f = idx - (double)lo;
   return v[lo] * (1 - f) + v[hi] * f;
+}
+
+void CUDART_CB slot_landed(void *arg) {
+  Slot *s = static_cast<Slot *>(arg);
+  cgx_server *sv = s->owner;
+  {
+    std::lock_guard<std::mutex> g(sv->mu);
+    s->landed = true;
+  }
+  sv->cv.notify_all();
 }
 
 } // namespace
@@ -300,6 +366,7 @@ int cgx_server_create(cgx_server **out, int mode, int64_t hbm_budget_bytes, int 
   sv->max_requests = (size_t)max_requests;
   sv->reqs.reserve(sv->max_requests);
   for (int i = 0; i < 2; ++i) {
+    sv->slots[i].owner = sv;
     int rc = slot_init(sv->slots[i], (size_t)max_pairs, (size_t)max_tiles);
     if (rc) {
       for (int j = 0; j <= i; ++j) slot_free(sv->slots[j]);
@@ -342,12 +409,11 @@ int cgx_server_release(cgx_server *sv, int64_t bytes) {
 
 int cgx_server_define_op(cgx_server *sv, int hier, const cgx_batch *pairs, int *op_id) {
   if (!sv || !op_id || hier < 0) return set_error(CGX_EINVAL, "bad operation");
-  if (sv->worker.joinable()) return set_error(CGX_EINVAL, "define operations before starting");
   const Desc *d;
   const int *nt;
-  const long long *pts;
+  const long long *pts, *byt;
   int n;
-  int rc = batch_pairs(pairs, &d, &nt, &pts, &n);
+  int rc = batch_pairs(pairs, &d, &nt, &pts, &byt, &n);
   if (rc) return rc;
   OpTemplate op;
   op.hier = hier;
@@ -357,9 +423,14 @@ int cgx_server_define_op(cgx_server *sv, int hier, const cgx_batch *pairs, int *
   for (int i = 0; i < n; ++i)
     if (is_stencil(op.descs[i].kind) && !encode_tma_maps(op.descs[i], &op.maps[3 * (size_t)i]))
       op.descs[i].bx = 0;
-  for (int i = 0; i < n; ++i) { op.tiles += nt[i]; op.points += pts[i]; }
+  for (int i = 0; i < n; ++i) {
+    op.tiles += nt[i];
+    op.points += pts[i];
+    op.bytes += byt[i];
+  }
   if (op.descs.size() > sv->slots[0].desc_cap || (size_t)op.tiles > sv->slots[0].tile_cap)
     return set_error(CGX_EINVAL, "operation larger than a server slot");
+  std::lock_guard<std::mutex> g(sv->mu); // the worker may be running
   sv->ops.push_back(std::move(op));
   if ((int)sv->hier_busy.size() <= hier) sv->hier_busy.resize(hier + 1, 0);
   *op_id = (int)sv->ops.size() - 1;
@@ -377,9 +448,10 @@ int cgx_server_start(cgx_server *sv) {
 }
 
 int cgx_server_submit(cgx_server *sv, int op_id, int64_t *request_id) {
-  if (!sv || op_id < 0 || op_id >= (int)sv->ops.size()) return set_error(CGX_EINVAL, "bad request");
+  if (!sv || op_id < 0) return set_error(CGX_EINVAL, "bad request");
   {
     std::lock_guard<std::mutex> g(sv->mu);
+    if (op_id >= (int)sv->ops.size()) return set_error(CGX_EINVAL, "bad request: no operation %d", op_id);
     if (sv->reqs.size() >= sv->max_requests)
       return set_error(CGX_ENOMEM, "request log full (%zu requests)", sv->max_requests);
     Request r;
@@ -422,13 +494,14 @@ int cgx_server_stats(cgx_server *sv, cgx_server_report *rep) {
   std::lock_guard<std::mutex> g(sv->mu);
   std::vector<double> lat;
   double first = 1e300, last = 0;
-  long long points = 0, done = 0;
+  long long points = 0, bytes = 0, done = 0;
   for (const Request &r : sv->reqs) {
     if (r.t_done <= 0) continue;
     lat.push_back(1e3 * (r.t_done - r.t_arrive));
     first = std::min(first, r.t_arrive);
     last = std::max(last, r.t_done);
     points += sv->ops[r.op].points;
+    bytes += sv->ops[r.op].bytes;
     ++done;
   }
   memset(rep, 0, sizeof *rep);
@@ -444,6 +517,8 @@ int cgx_server_stats(cgx_server *sv, cgx_server_report *rep) {
                                        (double)(sv->mode == CGX_SERVE_BATCHED ? sv->launches : done)
                                  : 0;
   rep->hbm_used = sv->used;
+  rep->bytes = bytes;
+  rep->bytes_per_s = rep->makespan_s > 0 ? (double)bytes / rep->makespan_s : 0;
   return CGX_OK;
 }
 

@@ -240,7 +240,12 @@ int cgx_graph_destroy(cgx_graph *g);
  * kernel on two alternating launch slots; a hierarchy's requests run one
  * after another in arrival order.  CGX_SERVE_PLAIN serves one request at a
  * time through per-box launches (the baseline).  Hierarchies are admitted
- * against an HBM budget with cgx_server_admit/release.
+ * against an HBM budget with cgx_server_admit/release; admission, release
+ * and cgx_server_define_op are allowed while the worker runs, so that a
+ * hierarchy admitted mid-stream is served from its first request on.  A
+ * launch's segments (prolongation, copy, restriction kernels) run
+ * concurrently on side streams of the slot.  The report's bytes are the
+ * algorithmic bytes of the completed requests.
  */
 #define CGX_SERVE_BATCHED 0
 #define CGX_SERVE_PLAIN 1
@@ -248,6 +253,8 @@ typedef struct cgx_server cgx_server;
 typedef struct cgx_server_report {
   int64_t requests, launches, fine_points, hbm_used;
   double p50_ms, p99_ms, mean_ms, makespan_s, points_per_s, mean_batch;
+  int64_t bytes;      /* algorithmic bytes of the completed requests */
+  double bytes_per_s; /* bytes / makespan */
 } cgx_server_report;
 int cgx_server_create(cgx_server **out, int mode, int64_t hbm_budget_bytes,
                       int max_pairs, int64_t max_tiles, int64_t max_requests);

@@ -5,8 +5,13 @@ server (cgx_server_* in include/cgx.h).
   the final grid data after a Poisson stream served batched is bit-for-bit
   the data after serving the same stream one request at a time through the
   per-box drop-in (every request alone, in order).
-* Admission refuses hierarchies beyond the HBM budget and admits again once
-  memory is released.
+* Per request: in rounds where every hierarchy receives exactly one request
+  (sync, prolongation, restriction or regrid fill), all of a round's
+  requests are served together in the mix and, separately, each alone; every
+  hierarchy's arrays -- that request's result -- agree bit for bit.
+* Admission refuses hierarchies beyond the HBM budget; once a hierarchy is
+  retired, a waiting one is admitted while the server runs, its operations
+  are defined mid-stream, and its requests are served as they would be alone.
 """
 import numpy as np
 import pytest
@@ -24,18 +29,24 @@ def cgx():
 
 
 def _state(ens):
-    return [p.clone() for m in ens.members for lp in m.storage.pools for p in lp]
+    return [p.clone() for m in range(len(ens.members)) if not ens.members[m].retired
+            for p in ens.state(m)]
+
+
+def _equal(xs, ys):
+    return len(xs) == len(ys) and all(torch.equal(a.view(torch.int64), b.view(torch.int64))
+                                      for a, b in zip(xs, ys))
 
 
 def test_batched_stream_equals_requests_alone(cgx):
     from carpet_b200.serve import (SERVE_BATCHED, SERVE_PLAIN, Ensemble, Server, ops_for,
                                    poisson_trace)
-    cgx.set_fp_mode(True)
+    cgx.set_fp_mode(False)
     batched = Server(mode=SERVE_BATCHED)
     plain = Server(mode=SERVE_PLAIN)
-    ens = Ensemble(batched, nhier=8, size_range=(24, 40), seed=11)
+    ens = Ensemble(batched, nhier=8, size_range=(24, 40), seed=11, regrid=True)
     plain_ops = ens.define(plain)
-    keys, arr = poisson_trace(ens, rate=1e5, n=300, seed=3)
+    keys, arr = poisson_trace(ens, rate=1e5, n=300, seed=3, mix=(0.55, 0.25, 0.15, 0.05))
     init = ens.snapshot()
     batched.replay(ops_for(ens.ops, keys), arr)
     batched.drain()
@@ -50,8 +61,42 @@ def test_batched_stream_equals_requests_alone(cgx):
     assert rb["launches"] < rp["launches"]          # batched: fewer, larger launches
     assert rb["mean_batch"] > 1.0                   # requests really overlapped
     assert 0 < rb["p50_ms"] <= rb["p99_ms"]
-    for a, b in zip(got, want):
-        assert torch.equal(a.view(torch.int64), b.view(torch.int64))
+    assert rb["bytes"] == rp["bytes"] > 0
+    assert _equal(got, want)
+    batched.close()
+    plain.close()
+
+
+def test_each_request_alone_equals_in_mix(cgx):
+    """rounds of one request per hierarchy: the round served as one burst
+    (continuously batched, requests of different hierarchies overlapping on
+    the GPU) against each request served alone"""
+    from carpet_b200.serve import SERVE_BATCHED, SERVE_PLAIN, Ensemble, Server, ops_for, request_key
+    cgx.set_fp_mode(False)
+    batched = Server(mode=SERVE_BATCHED)
+    plain = Server(mode=SERVE_PLAIN)
+    ens = Ensemble(batched, nhier=12, size_range=(24, 48), seed=21, regrid=True)
+    plain_ops = ens.define(plain)
+    rng = np.random.default_rng(5)
+    kinds = set()
+    for rnd in range(4):
+        keys = []
+        for m in range(len(ens.members)):
+            k = int(rng.integers(0, 4))
+            keys.append(request_key(ens, m, k, rng))
+            kinds.add(k)
+        before = ens.snapshot()
+        batched.replay(ops_for(ens.ops, keys), [0.0] * len(keys))  # one burst
+        batched.drain()
+        mix = [[p.clone() for p in ens.state(m)] for m in range(len(ens.members))]
+        ens.restore(before)
+        for key in keys:                                # each request alone
+            plain.submit(plain_ops[key])
+            plain.drain()
+        for m in range(len(ens.members)):
+            assert _equal(mix[m], ens.state(m)), (rnd, keys[m])
+    assert kinds == {0, 1, 2, 3}
+    assert batched.report()["mean_batch"] > 1.0
     batched.close()
     plain.close()
 
@@ -69,3 +114,43 @@ def test_admission_against_budget(cgx):
     ens.close()                      # releases the admitted hierarchies
     assert sv.admit(one) and sv.admit(one)
     sv.close()
+
+
+def test_admission_while_serving(cgx):
+    """a waiting hierarchy is admitted mid-stream after another retires; its
+    operations are defined on the running server and its requests give what
+    they give served alone"""
+    from carpet_b200.amr import storage_bytes
+    from carpet_b200.hierarchy import nested
+    from carpet_b200.serve import (SERVE_BATCHED, SERVE_PLAIN, Ensemble, Server, ops_for,
+                                   poisson_trace, request_key)
+    cgx.set_fp_mode(False)
+    h = nested(3, (25, 25, 25), parts=(2, 1, 1), ghost=3, buffer=3, order=5)
+    one = storage_bytes(h, 4, 3)
+    sv = Server(mode=SERVE_BATCHED, hbm_budget=int(3.5 * one))
+    plain = Server(mode=SERVE_PLAIN)
+    ens = Ensemble(sv, nhier=5, size_range=(24, 24), seed=7)
+    assert len(ens.members) == 3 and ens.deferred == 2
+    keys, arr = poisson_trace(ens, rate=2e4, n=120, seed=9)
+    sv.replay(ops_for(ens.ops, keys), arr)          # starts the worker
+    sv.drain()
+    ens.retire(0)                                   # its memory returns to the budget
+    new, (plain_ops,) = ens.admit_pending([plain])  # defined while sv runs
+    assert len(new) == 1 and ens.deferred == 1
+    m = new[0]
+    init = [p.clone() for p in ens.state(m)]
+    rng = np.random.default_rng(3)
+    mine = [request_key(ens, m, int(rng.integers(0, 3)), rng) for _ in range(20)]
+    others = [request_key(ens, 1 + i % 2, int(rng.integers(0, 3)), rng) for i in range(20)]
+    stream = [k for pair in zip(mine, others) for k in pair]
+    sv.replay(ops_for(ens.ops, stream), [1e-5 * i for i in range(len(stream))])
+    sv.drain()
+    got = [p.clone() for p in ens.state(m)]
+    for p, q in zip(ens.state(m), init):
+        p.copy_(q)
+    for k in mine:                                  # alone, one at a time
+        plain.submit(plain_ops[k])
+        plain.drain()
+    assert _equal(got, ens.state(m))
+    sv.close()
+    plain.close()
