@@ -23,8 +23,8 @@ cpu_baseline CarpetLib's own operators (compiled from the reference) on the
              host cores, a bounded sample of the same step
 served       the served ensemble (64 hierarchies, Poisson request stream)
 batched_uneven  256 uneven mixed box-pairs, autotuned + graph vs per box
-moving_boxes (--moving) the 8-level moving-box hierarchy: a coarse step and a
-             regrid (host schedule + batched graph fill)
+moving_boxes the 8-level moving-box hierarchy: a coarse step and a regrid
+             (host schedule + batched graph fill); --no-moving skips it
 
 --impl reference: only the CPU reference arm (rank 0).
 """
@@ -98,8 +98,8 @@ def parse():
     p.add_argument("--max-ctas", type=int, nargs=2, default=[0, 0], metavar=("TMA", "STREAM"),
                    help="CTAs per SM of the TMA prolongation and the streaming kernels (0: all that "
                         "fit); below the limit, the grid-function groups' kernels share the SMs")
-    p.add_argument("--moving", action="store_true",
-                   help="add the moving-box section (~80 GB on the device, minutes)")
+    p.add_argument("--no-moving", action="store_true",
+                   help="skip the moving-box section (8 levels, ~51 GB on the device)")
     return p.parse_args()
 
 
@@ -291,13 +291,15 @@ def cpu_reference(h, ngf, seconds_per_step, steps, warmup):
 
 
 # ----------------------------------------------------------------- served
-def served(seconds: float):
+def served(seconds: float, peak_gbs: float):
     """The served ensemble: 64 independent 3-level hierarchies (coarse sizes
     U{24..64} per axis, 4 grid functions x 3 timelevels, 2 components per
-    level), admitted against a 150 GB HBM budget; Poisson request streams
-    (sync/prolong/restrict 60/25/15) at 1e3, 1e4 and 1e5 requests/s, each
-    served continuously batched and, at the lower rates, through the plain
-    per-box drop-in one request at a time."""
+    level, each with a regrid-fill operation), admitted against a 150 GB HBM
+    budget.  Poisson request streams (sync/prolong/restrict 60/25/15) at 1e3,
+    1e4 and 1e5 requests/s, each served continuously batched and through the
+    plain per-box drop-in one request at a time; a stream with 5% regrid
+    fills; and the closed-loop saturation point (every request submitted at
+    once), with its algorithmic GB/s against the HBM roof."""
     import torch
     from carpet_b200.serve import (SERVE_BATCHED, SERVE_PLAIN, Ensemble, Server, ops_for,
                                    poisson_trace)
@@ -305,7 +307,7 @@ def served(seconds: float):
                        "order-5 prolongation + 3-TL time interpolation; Poisson stream "
                        "sync/prolong/restrict 60/25/15", "budget_gb": 150, "rates": []}
     warm = Server(mode=SERVE_BATCHED)
-    ens = Ensemble(warm, nhier=64, size_range=(24, 64), seed=42)
+    ens = Ensemble(warm, nhier=64, size_range=(24, 64), seed=42, regrid=True)
     plain = Server(mode=SERVE_PLAIN)
     plain_ops = ens.define(plain)
     keys, arr = poisson_trace(ens, 1e4, 200, seed=1)   # warm-up: module load, attributes
@@ -316,24 +318,41 @@ def served(seconds: float):
     plain.close()
     out["hierarchies"] = len(ens.members)
     out["hbm_gb"] = round(warm.report()["hbm_used"] / 1e9, 3)
+
+    def run(mode, keys, arr):
+        sv = Server(mode=mode)
+        op_ids = ens.define(sv)
+        torch.cuda.synchronize()
+        sv.replay(ops_for(op_ids, keys), arr)
+        sv.drain()
+        r = sv.report()
+        sv.close()
+        return {"requests": int(r["requests"]), "p50_ms": round(r["p50_ms"], 4),
+                "p99_ms": round(r["p99_ms"], 4),
+                "fine_points_per_s": round(r["points_per_s"], 1),
+                "gbs": round(r["bytes_per_s"] / 1e9, 2),
+                "launches": r["launches"], "mean_batch": round(r["mean_batch"], 2)}
+
     for rate in (1e3, 1e4, 1e5):
         n = int(min(rate * seconds, 20000))
         keys, arr = poisson_trace(ens, rate, n, seed=int(rate))
-        row = {"rate_per_s": rate, "requests": n}
-        for mode, name in ((SERVE_BATCHED, "batched"), (SERVE_PLAIN, "plain")):
-            if mode == SERVE_PLAIN and rate > 1e4:
-                continue  # the plain drop-in falls behind without bound at 1e5/s
-            sv = Server(mode=mode)
-            op_ids = ens.define(sv)
-            torch.cuda.synchronize()
-            sv.replay(ops_for(op_ids, keys), arr)
-            sv.drain()
-            r = sv.report()
-            row[name] = {"p50_ms": round(r["p50_ms"], 4), "p99_ms": round(r["p99_ms"], 4),
-                         "fine_points_per_s": round(r["points_per_s"], 1),
-                         "launches": r["launches"], "mean_batch": round(r["mean_batch"], 2)}
-            sv.close()
+        row = {"rate_per_s": rate, "requests": n, "batched": run(SERVE_BATCHED, keys, arr)}
+        # the plain drop-in falls behind at the highest rate: a bounded prefix
+        m = n if rate <= 1e4 else min(n, 4000)
+        row["plain"] = run(SERVE_PLAIN, keys[:m], arr[:m])
         out["rates"].append(row)
+    keys, arr = poisson_trace(ens, 1e4, int(min(1e4 * seconds, 10000)), seed=77,
+                              mix=(0.57, 0.24, 0.14, 0.05))
+    out["with_regrid_fill"] = {"rate_per_s": 1e4, "mix": "sync/prolong/restrict/regrid-fill 57/24/14/5",
+                               "batched": run(SERVE_BATCHED, keys, arr),
+                               "plain": run(SERVE_PLAIN, keys, arr)}
+    # closed loop: the whole stream submitted at once
+    keys, _ = poisson_trace(ens, 1e5, 20000, seed=99)
+    sat = {"requests": len(keys), "batched": run(SERVE_BATCHED, keys, [0.0] * len(keys)),
+           "plain": run(SERVE_PLAIN, keys[:2000], [0.0] * 2000)}
+    sat["batched"]["frac_hbm_roof"] = round(sat["batched"]["gbs"] / peak_gbs, 4)
+    sat["batched_vs_plain"] = round(sat["batched"]["gbs"] / max(1e-9, sat["plain"]["gbs"]), 1)
+    out["saturation"] = sat
     warm.close()
     return out
 
@@ -386,7 +405,7 @@ def uneven(steps: int, warmup: int, fp: str):
 
 
 # ----------------------------------------------------------------- moving
-def moving(ngf: int, fp: str, steps: int):
+def moving(ngf: int, fp: str, steps: int, peak_gbs: float):
     """Moving-box configuration: 8 vertex-centred levels (a 257^3 coarse level
     in 16 components; 7 refined levels of two 161^3 boxes, 8 components each,
     around two centres orbiting at 0.3 L, one revolution per 256 coarse
@@ -458,6 +477,8 @@ def moving(ngf: int, fp: str, steps: int):
            "regrid_alloc_ms": round((t1 - tb) * 1e3, 1),
            "regrid_fill_ms": round(fill_ms, 3),
            "regrid_fill_gbs": round(rst["bytes"] / (fill_ms * 1e-3) / 1e9, 1),
+           "step_frac_hbm_roof": round(sst["bytes"] / (step_ms * 1e-3) / 1e9 / peak_gbs, 4),
+           "fill_frac_hbm_roof": round(rst["bytes"] / (fill_ms * 1e-3) / 1e9 / peak_gbs, 4),
            "regrid_pairs": rst["pairs"], "regrid_fine_points": rst["points"],
            "tile_configs": sorted({c for v in tuned.values() for c in v.values()})}
     del gr
@@ -750,15 +771,15 @@ def main():
 
     serve = None
     if rank == 0 and not args.no_serve:
-        serve = served(args.serve_seconds)
+        serve = served(args.serve_seconds, peak)
 
     batched_uneven = None
     if rank == 0 and not args.no_uneven:
         batched_uneven = uneven(max(args.steps, 3), args.warmup, args.fp)
 
     moving_boxes = None
-    if rank == 0 and args.moving:
-        moving_boxes = moving(args.ngf, args.fp, 2)
+    if rank == 0 and not args.no_moving:
+        moving_boxes = moving(args.ngf, args.fp, 2, peak)
 
     # DRAM bytes per launch of the dominant kernel: the ratio of DRAM bytes
     # to algorithmic bytes that ncu measured on a smaller capture of the same

@@ -53,6 +53,9 @@ struct OpTemplate {
   std::vector<CUtensorMap> maps; // 3 per descriptor (prolongation staged by TMA)
   std::vector<int> ntiles;
   long long tiles = 0, points = 0, bytes = 0;
+  // the operation's tiles by tile-map segment, (descriptor within the
+  // operation, tile): a launch concatenates these with descriptor offsets
+  std::vector<int2> seg_tiles[NSEG];
 };
 
 struct Request {
@@ -74,10 +77,7 @@ struct Slot {
   size_t desc_cap = 0, tile_cap = 0;
   bool busy = false;
   std::vector<int> reqs;
-  // set by the host function enqueued behind the slot's launch (a CUDA
-  // driver thread), read by the worker under the server's mutex
-  bool landed = false;
-  struct cgx_server *owner = nullptr;
+  long long seq = 0; // launch order of the slot's current work
 };
 
 } // namespace
@@ -112,7 +112,8 @@ namespace {
 
 int slot_init(Slot &s, size_t desc_cap, size_t tile_cap) {
   cudaError_t e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
+  // blocking sync: a worker that waits on it sleeps instead of spinning
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming | cudaEventBlockingSync);
   if (e == cudaSuccess) e = cudaMalloc(&s.d_descs, desc_cap * sizeof(Desc));
   if (e == cudaSuccess) e = cudaMallocHost(&s.h_descs, desc_cap * sizeof(Desc));
   if (e == cudaSuccess) e = cudaMalloc(&s.d_maps, 3 * desc_cap * sizeof(CUtensorMap));
@@ -153,9 +154,6 @@ void slot_free(Slot &s) {
   s = Slot();
 }
 
-// Host function behind a slot's launch: wakes the worker (no CUDA calls).
-void CUDART_CB slot_landed(void *arg);
-
 // Retire a slot whose kernel has finished.
 void retire(cgx_server *sv, Slot &s) {
   const double t = sv->now();
@@ -167,7 +165,6 @@ void retire(cgx_server *sv, Slot &s) {
   sv->completed += (long long)s.reqs.size();
   s.reqs.clear();
   s.busy = false;
-  s.landed = false;
   sv->cv.notify_all();
 }
 
@@ -213,22 +210,21 @@ bool launch_batch(cgx_server *sv, Slot &s) {
   // variant's), one persistent kernel per segment
   size_t di = 0, ti = 0;
   const double t = sv->now();
+  std::vector<int> base(take.size());
   for (size_t q = 0; q < take.size(); ++q) {
     const OpTemplate &op = *tops[q];
-    for (size_t k = 0; k < op.descs.size(); ++k) {
-      for (int j = 0; j < 3; ++j) s.h_maps[3 * di + j] = op.maps[3 * k + j];
-      s.h_descs[di++] = op.descs[k];
-    }
+    const size_t n = op.descs.size();
+    memcpy(s.h_descs + di, op.descs.data(), n * sizeof(Desc));
+    memcpy(s.h_maps + 3 * di, op.maps.data(), 3 * n * sizeof(CUtensorMap));
+    base[q] = (int)di;
+    di += n;
     sv->reqs[take[q]].t_launch = t;
   }
   long long seg[NSEG + 1];
   for (int g = 0; g < NSEG; ++g) {
     seg[g] = (long long)ti;
-    size_t d0 = 0;
-    for (const OpTemplate *op : tops)
-      for (size_t k = 0; k < op->descs.size(); ++k, ++d0)
-        if (segment_of(op->descs[k]) == g)
-          for (int j = 0; j < op->ntiles[k]; ++j) s.h_tmap[ti++] = make_int2((int)d0, j);
+    for (size_t q = 0; q < take.size(); ++q)
+      for (const int2 &e : tops[q]->seg_tiles[g]) s.h_tmap[ti++] = make_int2(e.x + base[q], e.y);
   }
   seg[NSEG] = (long long)ti;
   cudaError_t e = cudaMemcpyAsync(s.d_descs, s.h_descs, di * sizeof(Desc), cudaMemcpyHostToDevice, s.stream);
@@ -247,10 +243,10 @@ bool launch_batch(cgx_server *sv, Slot &s) {
   }
   if (rc) sv->error = rc;
   e = cudaEventRecord(s.done, s.stream);
-  if (e == cudaSuccess) e = cudaLaunchHostFunc(s.stream, slot_landed, &s);
-  if (e != cudaSuccess && !sv->error) sv->error = cuda_error(e, "slot completion");
+  if (e != cudaSuccess && !sv->error) sv->error = cuda_error(e, "cudaEventRecord");
   s.reqs = take;
   s.busy = true;
+  s.seq = sv->launches;
   sv->launches++;
   sv->batched_requests += (long long)take.size();
   return true;
@@ -274,10 +270,10 @@ bool launch_plain(cgx_server *sv, Slot &s) {
     if (rc) sv->error = rc;
   }
   cudaError_t e = cudaEventRecord(s.done, s.stream);
-  if (e == cudaSuccess) e = cudaLaunchHostFunc(s.stream, slot_landed, &s);
-  if (e != cudaSuccess && !sv->error) sv->error = cuda_error(e, "slot completion");
+  if (e != cudaSuccess && !sv->error) sv->error = cuda_error(e, "cudaEventRecord");
   s.reqs.assign(1, r);
   s.busy = true;
+  s.seq = sv->launches;
   sv->launches += (long long)op.descs.size();
   sv->batched_requests += 1;
   return true;
@@ -309,18 +305,23 @@ void worker_loop(cgx_server *sv) {
       if (sv->pending.empty()) return;
     }
     if (any_busy) {
-      // sleep until a slot's launch lands (its host function notifies) or
-      // a request arrives that a free slot could take; the bound only
-      // guards against a missed notification
-      std::unique_lock<std::mutex> g(sv->mu);
-      sv->cv.wait_for(g, std::chrono::milliseconds(2), [&] {
-        bool landed = false, free_slot = false;
-        for (int i = 0; i < nslots; ++i) {
-          landed |= sv->slots[i].busy && sv->slots[i].landed;
-          free_slot |= !sv->slots[i].busy;
-        }
-        return landed || (free_slot && !sv->pending.empty()) || sv->stop.load();
-      });
+      bool all_busy = true;
+      int oldest = -1;
+      for (int i = 0; i < nslots; ++i) {
+        all_busy &= sv->slots[i].busy;
+        if (sv->slots[i].busy && (oldest < 0 || sv->slots[i].seq < sv->slots[oldest].seq)) oldest = i;
+      }
+      if (all_busy) {
+        // nothing can launch before a slot frees: sleep on the oldest
+        // slot's blocking-sync event (no core spins meanwhile)
+        cudaEventSynchronize(sv->slots[oldest].done);
+      } else {
+        // a free slot and nothing pending: wake for a new request or,
+        // after a short while, to poll the busy slot again
+        std::unique_lock<std::mutex> g(sv->mu);
+        sv->cv.wait_for(g, std::chrono::microseconds(20),
+                        [&] { return !sv->pending.empty() || sv->stop.load(); });
+      }
     } else {
       std::unique_lock<std::mutex> g(sv->mu);
       sv->cv.wait_for(g, std::chrono::microseconds(200),
@@ -337,16 +338,6 @@ double percentile(std::vector<double> v, double p) {
   size_t hi = std::min(lo + 1, v.size() - 1);
   double f = idx - (double)lo;
   return v[lo] * (1 - f) + v[hi] * f;
-}
-
-void CUDART_CB slot_landed(void *arg) {
-  Slot *s = static_cast<Slot *>(arg);
-  cgx_server *sv = s->owner;
-  {
-    std::lock_guard<std::mutex> g(sv->mu);
-    s->landed = true;
-  }
-  sv->cv.notify_all();
 }
 
 } // namespace
@@ -366,7 +357,6 @@ int cgx_server_create(cgx_server **out, int mode, int64_t hbm_budget_bytes, int 
   sv->max_requests = (size_t)max_requests;
   sv->reqs.reserve(sv->max_requests);
   for (int i = 0; i < 2; ++i) {
-    sv->slots[i].owner = sv;
     int rc = slot_init(sv->slots[i], (size_t)max_pairs, (size_t)max_tiles);
     if (rc) {
       for (int j = 0; j <= i; ++j) slot_free(sv->slots[j]);
@@ -427,6 +417,8 @@ int cgx_server_define_op(cgx_server *sv, int hier, const cgx_batch *pairs, int *
     op.tiles += nt[i];
     op.points += pts[i];
     op.bytes += byt[i];
+    std::vector<int2> &st = op.seg_tiles[segment_of(op.descs[i])];
+    for (int j = 0; j < nt[i]; ++j) st.push_back(make_int2(i, j));
   }
   if (op.descs.size() > sv->slots[0].desc_cap || (size_t)op.tiles > sv->slots[0].tile_cap)
     return set_error(CGX_EINVAL, "operation larger than a server slot");
