@@ -151,11 +151,20 @@ def build_level(box: Box, parts, ghost: int) -> Level:
 
 
 def nested(nlevels: int, npoints, parts=(2, 2, 2), ghost=3, buffer=9, order=5,
-           origin=(0, 0, 0), native: bool = True) -> Hierarchy:
+           origin=(0, 0, 0), native: bool = True, schedule: str = "regular") -> Hierarchy:
     """``nlevels`` vertex-centred levels of ``npoints`` points per axis each
     (an int or one per axis, each 1 mod 4), each level covering the central
     half of the next coarser one; ``parts`` splits every level into
-    components (one (px, py, pz) for all levels, or a list of one per level)."""
+    components (one (px, py, pz) for all levels, or a list of one per level).
+
+    ``schedule``: "regular" -- this module's region lists for box
+    hierarchies (the C++ ``cgx_sched_*`` with ``native``, else the Python
+    restatement); "dh" -- CarpetLib's own region algebra for the same
+    arrays (``carpet_b200.dh``: internal ghost points in a refined level's
+    outer ghost layer are boundary-prolongated rather than synced, and
+    restriction also fills the coarse ghost zones), which needs the levels
+    properly nested (every refined level inside the next coarser level's
+    active region with its stencils)."""
     n = (npoints,) * 3 if isinstance(npoints, int) else tuple(npoints)
     assert all((m - 1) % 4 == 0 for m in n)
     st0 = 2 ** (nlevels - 1)
@@ -169,7 +178,17 @@ def nested(nlevels: int, npoints, parts=(2, 2, 2), ghost=3, buffer=9, order=5,
         # next level: the central half, (n-1)/4 coarse points in
         lo = [lo[d] + ((n[d] - 1) // 4) * st for d in range(3)]
     h = Hierarchy(levels, ghost, buffer, order)
-    schedule(h, native)
+    if schedule == "dh":
+        from . import dh
+        doms, ints = dh.from_nested(h)
+        g = (dh.schedule if native else dh.schedule_py)(doms, ints, ghost, buffer, order)
+        for l in range(nlevels):
+            assert [c.exterior for c in g.levels[l].comps] == [c.exterior for c in h.levels[l].comps]
+        h.sync, h.prolong, h.restrict = g.sync, g.prolong, g.restrict
+        return h
+    if schedule != "regular":
+        raise ValueError(f"unknown schedule {schedule!r}")
+    globals()["schedule"](h, native)
     return h
 
 

@@ -216,6 +216,39 @@ int cgx_sched_old2new(int nnew, const int *new_exterior, int nold, const int *ol
                       const int *cinterior, const int *cexterior, int order, cgx_pair_box *copies,
                       int max_copies, int *ncopies, cgx_pair_box *prols, int max_prols, int *nprols);
 
+/*
+ * The dh schedule producer for arbitrary component sets: the region algebra
+ * of dh::regrid (CarpetLib/src/dh.cc:300-1088) for vertex-centred
+ * hierarchies with refinement factor 2.  Input per level l: its domain
+ * (h.baseextent: the whole domain at the level's stride, domains[9 l ..])
+ * and its ncomps[l] component interiors (disjoint boxes, consecutive in
+ * interiors[]).  Each component's exterior is its interior grown by `ghost`
+ * on faces off the domain boundary; boundary_width points of the domain
+ * boundary are outer boundary; buffer zones are the owned points within
+ * `buffer` of the level's not-owned region.  Schedules (cgx_dh_pairs):
+ *   CGX_DH_SYNC     level l's ghost zones from its other components'
+ *                   interiors (dh.cc:837-894);
+ *   CGX_DH_BNDPROL  what sync leaves, and the buffer zones, of level l from
+ *                   level l-1, send boxes grown by order/2 (dh.cc:896-977);
+ *   CGX_DH_RESTRICT the points of level l under level l+1's active region
+ *                   from level l+1, into every component's exterior
+ *                   (restrict_into_ghosts, CarpetLib's default) or interior
+ *                   (dh.cc:981-1088).
+ * Every point is received once, from the component the reference's order
+ * picks; the reference's consistency checks return CGX_EINVAL.
+ */
+#define CGX_DH_SYNC 0
+#define CGX_DH_BNDPROL 1
+#define CGX_DH_RESTRICT 2
+typedef struct cgx_dh cgx_dh;
+int cgx_dh_create(cgx_dh **out, int nlevels, const int *domains, const int *ncomps, const int *interiors,
+                  int ghost, int buffer, int boundary_width, int order, int restrict_into_ghosts);
+int cgx_dh_destroy(cgx_dh *h);
+/* the ncomps[level] component exteriors, 9 ints each */
+int cgx_dh_exteriors(const cgx_dh *h, int level, int *out);
+/* a schedule of `level`; *n is its length (CGX_EINVAL when above max) */
+int cgx_dh_pairs(const cgx_dh *h, int level, int kind, cgx_pair_box *out, int max, int *n);
+
 /* device status word of the last launches: 0 or a CGX_E* code */
 int cgx_batch_check(cgx_batch *b, void *stream);
 

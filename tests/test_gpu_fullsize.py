@@ -17,7 +17,14 @@ injection and ghost sync -- one coarse Berger-Oliger step, FMA mode.
 * the grid functions split into groups whose phase chains run on separate
   streams (eagerly and captured as one graph, the groups started together
   or staggered by whole phases) give the same bits as one chain over all
-  of them.
+  of them;
+* with CarpetLib's own region lists (carpet_b200.dh: the outer ghost
+  layer's internal ghost points prolongated instead of synced, restriction
+  into the coarse ghost zones too) the step matches the oracle's replay of
+  those lists, and gives the same bits as the box hierarchy's lists: a
+  prolongated point and a synced copy of a prolongated point are the same
+  value, and so are a restricted ghost point and the sync that overwrites
+  it.
 """
 import numpy as np
 import pytest
@@ -39,11 +46,11 @@ def cgx():
     return cb
 
 
-def workload(cb, ngf, fill, groups=1):
+def workload(cb, ngf, fill, groups=1, schedule="regular", fma=True):
     from carpet_b200.amr import BergerOliger, Storage
     from carpet_b200.hierarchy import nested
-    cb.set_fp_mode(True)
-    h = nested(LEVELS, NPOINTS, ghost=3, buffer=9, order=5)
+    cb.set_fp_mode(fma)
+    h = nested(LEVELS, NPOINTS, ghost=3, buffer=9, order=5, schedule=schedule)
     st = Storage(h, ngf, 3)
     fill(st, h)
     bo = BergerOliger(h, st, order_space=5, order_time=2, groups=groups)
@@ -56,6 +63,29 @@ def random_fill(st, h):
     for lp in st.pools:
         for p in lp:
             p.normal_(generator=gen)
+
+
+def consistent_fill(st, h):
+    """random values that are a function of the global point: every ghost
+    zone holds its neighbours' values, as in any state a run reaches (the
+    schedules may then take a point from either component)"""
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(11)
+    for lp in st.pools:  # padding and the gaps between arrays: zero in every storage
+        for p in lp:
+            p.zero_()
+    for l, lev in enumerate(h.levels):
+        box = lev.box
+        n = [(box[3 + d] - box[d]) // box[6 + d] + 1 for d in range(3)]
+        for tl in range(st.ntl):
+            for g in range(st.ngf):
+                G = torch.randn((n[2], n[1], n[0]), generator=gen, device="cuda", dtype=torch.float64)
+                for c, comp in enumerate(lev.comps):
+                    e = comp.exterior
+                    o = [(e[d] - box[d]) // box[6 + d] for d in range(3)]
+                    m = [(e[3 + d] - e[d]) // e[6 + d] + 1 for d in range(3)]
+                    st.data[l][tl][g][c].tensor[:, :, :m[0]] = \
+                        G[o[2]:o[2] + m[2], o[1]:o[1] + m[1], o[0]:o[0] + m[0]]
 
 
 def cubic_fill(st, h):
@@ -85,7 +115,7 @@ def host_copy(st, gfs):
                 for l in range(len(st.data))] for g in gfs}
 
 
-def oracle_phase(port, h, arr, key):
+def oracle_phase(port, h, arr, key, fma=True):
     """one phase of BergerOliger on one grid function's host arrays
     arr[level][pool][comp], in the batches' own terms (carpet_b200.amr)"""
     kind, l, rots, ntl = key
@@ -97,7 +127,7 @@ def oracle_phase(port, h, arr, key):
         for p in h.sync[l]:
             port.transfer(OP_LAGRANGE, VERTEX, a[p.dst_comp], ext(l, p.dst_comp), [a[p.src_comp]],
                           ext(l, p.src_comp), [0.0], list(p.dstbox), list(p.srcbox), 0.0, 1, 0,
-                          fma=True)
+                          fma=fma)
     elif kind == "prolong":
         rf, rc = rots
         dst = arr[l][pool(rf, 0)]
@@ -107,19 +137,20 @@ def oracle_phase(port, h, arr, key):
         for p in h.prolong[l]:
             port.transfer(OP_LAGRANGE, VERTEX, dst[p.dst_comp], ext(l, p.dst_comp),
                           [s[p.src_comp] for s in srcs], ext(l - 1, p.src_comp), times,
-                          list(p.dstbox), list(p.srcbox), time, 5, 2, fma=True)
+                          list(p.dstbox), list(p.srcbox), time, 5, 2, fma=fma)
     else:
         rc, rf = rots
         dst, src = arr[l][pool(rc, 0)], arr[l + 1][pool(rf, 0)]
         for p in h.restrict[l + 1]:
             port.transfer(OP_LAGRANGE, VERTEX, dst[p.dst_comp], ext(l, p.dst_comp),
                           [src[p.src_comp]], ext(l + 1, p.src_comp), [0.0], list(p.dstbox),
-                          list(p.srcbox), 0.0, 5, 0, fma=True)
+                          list(p.srcbox), 0.0, 5, 0, fma=fma)
 
 
-def test_bench_step_matches_oracle_on_sampled_grid_functions(cgx, port):
-    ngf = 25
-    h, st, bo = workload(cgx, ngf, random_fill)
+@pytest.mark.parametrize("schedule,fma", [("regular", True), ("dh", False)])
+def test_bench_step_matches_oracle_on_sampled_grid_functions(cgx, port, schedule, fma):
+    ngf = 25 if schedule == "regular" else 4
+    h, st, bo = workload(cgx, ngf, random_fill, schedule=schedule, fma=fma)
     gfs = (0, ngf - 1)
     want = host_copy(st, gfs)
     keys = bo.step_phases()
@@ -130,7 +161,7 @@ def test_bench_step_matches_oracle_on_sampled_grid_functions(cgx, port):
     got = host_copy(st, gfs)
     for g in gfs:
         for k in keys:
-            oracle_phase(port, h, want[g], k)
+            oracle_phase(port, h, want[g], k, fma=fma)
         for l in range(LEVELS):
             for p in range(3):
                 for c, a in enumerate(want[g][l][p]):
@@ -204,3 +235,17 @@ def test_grid_function_groups_on_streams_match_one_chain(cgx, groups, stagger):
         for a, b in zip(p1, p2):
             assert torch.equal(a.view(torch.int64), b.view(torch.int64)), ("level", l)
     del g
+
+
+def test_dh_lists_and_box_lists_give_the_same_step(cgx):
+    _, s1, b1 = workload(cgx, 3, consistent_fill, fma=False)
+    _, s2, b2 = workload(cgx, 3, consistent_fill, schedule="dh", fma=False)
+    for _ in range(2):
+        b1.run(b1.step_phases())
+        b2.run(b2.step_phases())
+    for b in list(b1.batches.values()) + list(b2.batches.values()):
+        b.check()
+    torch.cuda.synchronize()
+    for l, (p1, p2) in enumerate(zip(s1.pools, s2.pools)):
+        for a, b in zip(p1, p2):
+            assert torch.equal(a.view(torch.int64), b.view(torch.int64)), ("level", l)
