@@ -792,6 +792,26 @@ def main():
     except (OSError, ValueError, KeyError):
         traffic = None
 
+    # parity statement: the exact mode is bit-exact with the reference's
+    # operation order (tests compare bit patterns); the fused mode's error
+    # per operator is the table tests/test_gpu_fma_error.py measured
+    parity = {"fp_mode": args.fp,
+              "vs_reference": "bit-exact with CarpetLib compiled without contraction "
+                              "(tests/test_gpu_parity.py, tests/test_gpu_fullsize.py)"
+              if args.fp == "exact" else
+              "fused multiply-adds in the reference's order; |delta| per operator below"}
+    try:
+        tab = json.load(open(os.path.join(ROOT, "profiles", "fma_error_per_operator.json")))
+        rows = tab["operators"]
+        parity["fma_mode_error"] = {
+            "source": tab["command"],
+            "max_abs_over_eps_max_src": round(max(r["max_rel_eps_src"] for r in rows.values()), 3),
+            "max_ulp": max(r["max_ulp"] for r in rows.values()),
+            "per_operator": {k: [round(r["max_rel_eps_src"], 3), r["max_ulp"]] for k, r in rows.items()},
+            "per_operator_key": "[max |fma - exact| / (eps max|source|), max per-point ulp]"}
+    except (OSError, ValueError, KeyError):
+        pass
+
     if rank == 0:
         out = {
             "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
@@ -815,7 +835,7 @@ def main():
                          "launch": f"one launch over all {args.ngf} grid functions, timed alone",
                          "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks
                          else "fallback 6650 GB/s"},
-            "phases": phases,
+            "phases": phases, "parity": parity,
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(), "served": serve,
             "batched_uneven": batched_uneven, "moving_boxes": moving_boxes,
         }

@@ -159,4 +159,12 @@ def test_fma_error_per_operator(cgx):
     path = os.environ.get("CGX_ERROR_TABLE")
     if path:
         with open(path, "w") as f:
-            json.dump(table, f, indent=1)
+            json.dump({"command": "CGX_ERROR_TABLE=<path> python -m pytest "
+                                  "tests/test_gpu_fma_error.py -m gpu (B200)",
+                       "reference": "the oracle's exact mode, bit-identical with CarpetLib compiled "
+                                    "without contraction",
+                       "columns": {"max_abs": "max |fma - exact|",
+                                   "max_rel_eps_src": "max |fma - exact| / (eps max|source|)",
+                                   "max_ulp": "max |fma - exact| in units of the exact value's ulp",
+                                   "frac_differing": "fraction of points whose bits differ"},
+                       "operators": table}, f, indent=1)
