@@ -4,15 +4,19 @@
 // A request names an operation template -- the box-pairs of one transfer
 // (a sync, a boundary prolongation or a restriction of one level of one
 // hierarchy, over all of its grid functions) -- defined once from a
-// cgx_batch.  The worker thread keeps two launch slots.  Whenever a slot is
-// free it takes, in arrival order, the oldest pending request of every
-// hierarchy that has no request on the GPU, concatenates their descriptors
-// into one tile map and launches the persistent kernel on that slot's
-// stream; requests that arrive meanwhile wait only for the next free slot,
-// and the two slots' kernels overlap on the device.  A hierarchy never has
-// two requests in flight, so each hierarchy sees its requests applied one
-// after another in arrival order -- the results are those of running them
-// alone (tests/test_gpu_serving.py).
+// cgx_batch.  An operation's descriptors and tensor maps are uploaded once,
+// into a device pool that every launch reads, and its tiles are kept as
+// (pool descriptor, tile) entries by segment; a launch only concatenates
+// those entries into one tile map.  The worker thread keeps two launch
+// slots.  Whenever a slot is free it takes, in arrival order, the oldest
+// pending request of every hierarchy (one request per hierarchy per launch)
+// and launches the persistent kernels on that slot's stream.  A hierarchy
+// whose previous request is still in flight on the other slot may be taken:
+// the slot's stream then waits for the other slot's completion event before
+// its kernels, so each hierarchy sees its requests applied one after another
+// in arrival order -- the results are those of running them alone
+// (tests/test_gpu_serving.py) -- while the host prepares one slot as the
+// device runs the other.
 //
 // The plain mode serves the same stream through the per-box drop-in: one
 // request at a time, one kernel launch per box-pair.
@@ -49,12 +53,11 @@ using clk = std::chrono::steady_clock;
 
 struct OpTemplate {
   int hier;
-  std::vector<Desc> descs;
-  std::vector<CUtensorMap> maps; // 3 per descriptor (prolongation staged by TMA)
+  std::vector<Desc> descs; // host copies: the plain mode's per-box launches
   std::vector<int> ntiles;
   long long tiles = 0, points = 0, bytes = 0;
-  // the operation's tiles by tile-map segment, (descriptor within the
-  // operation, tile): a launch concatenates these with descriptor offsets
+  // the operation's tiles by tile-map segment, (descriptor in the server's
+  // device pool, tile): a launch concatenates these
   std::vector<int2> seg_tiles[NSEG];
 };
 
@@ -69,15 +72,24 @@ struct Slot {
   // the concurrent segment launch: side streams, fork and join events
   cudaStream_t side[CONCURRENT_SIDE_MAX] = {};
   cudaEvent_t ev[CONCURRENT_SIDE_MAX + 1] = {};
-  Desc *d_descs = nullptr, *h_descs = nullptr;
   int2 *d_tmap = nullptr, *h_tmap = nullptr;
-  CUtensorMap *d_maps = nullptr, *h_maps = nullptr;
   unsigned long long *d_counter = nullptr;
   int *d_status = nullptr;
-  size_t desc_cap = 0, tile_cap = 0;
+  size_t tile_cap = 0;
   bool busy = false;
   std::vector<int> reqs;
   long long seq = 0; // launch order of the slot's current work
+};
+
+// Every operation's descriptors and tensor maps (3 per descriptor), in
+// device memory for the server's lifetime.  Growing the pool copies it into
+// a larger allocation; the old one stays allocated (launches in flight read
+// it) until the server is destroyed.
+struct Pool {
+  Desc *descs = nullptr;
+  CUtensorMap *maps = nullptr;
+  size_t used = 0, cap = 0;
+  std::vector<void *> old; // superseded allocations
 };
 
 } // namespace
@@ -92,8 +104,11 @@ struct cgx_server {
   std::deque<OpTemplate> ops;
   std::vector<Request> reqs; // reserved at creation: never reallocated
   size_t max_requests = 0;
-  std::vector<char> hier_busy;
+  // per hierarchy: whether a request of it is in flight on slot 0 / slot 1
+  std::vector<unsigned char> hier_in[2];
   std::deque<int> pending;
+  Pool pool;             // grows under define_mu, read by the worker under mu
+  std::mutex define_mu;  // serialises cgx_server_define_op
   std::mutex mu;
   std::condition_variable cv;
   std::thread worker;
@@ -110,14 +125,10 @@ struct cgx_server {
 
 namespace {
 
-int slot_init(Slot &s, size_t desc_cap, size_t tile_cap) {
+int slot_init(Slot &s, size_t tile_cap) {
   cudaError_t e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
   // blocking sync: a worker that waits on it sleeps instead of spinning
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming | cudaEventBlockingSync);
-  if (e == cudaSuccess) e = cudaMalloc(&s.d_descs, desc_cap * sizeof(Desc));
-  if (e == cudaSuccess) e = cudaMallocHost(&s.h_descs, desc_cap * sizeof(Desc));
-  if (e == cudaSuccess) e = cudaMalloc(&s.d_maps, 3 * desc_cap * sizeof(CUtensorMap));
-  if (e == cudaSuccess) e = cudaMallocHost(&s.h_maps, 3 * desc_cap * sizeof(CUtensorMap));
   if (e == cudaSuccess) e = cudaMalloc(&s.d_tmap, tile_cap * sizeof(int2));
   if (e == cudaSuccess) e = cudaMallocHost(&s.h_tmap, tile_cap * sizeof(int2));
   // claim counters and exit counts (cgx_kernels.cuh, claims_done)
@@ -130,19 +141,50 @@ int slot_init(Slot &s, size_t desc_cap, size_t tile_cap) {
   for (int k = 0; k <= CONCURRENT_SIDE_MAX && e == cudaSuccess; ++k)
     e = cudaEventCreateWithFlags(&s.ev[k], cudaEventDisableTiming);
   if (e != cudaSuccess) return cuda_error(e, "server slot allocation");
-  s.desc_cap = desc_cap;
   s.tile_cap = tile_cap;
   return CGX_OK;
 }
 
+// The descriptor pool with room for at least `need` descriptors (called
+// under define_mu; publishes a new pool under mu).
+int pool_reserve(cgx_server *sv, size_t need) {
+  Pool &p = sv->pool;
+  if (need <= p.cap) return CGX_OK;
+  size_t cap = std::max<size_t>(p.cap ? 2 * p.cap : 4096, need);
+  Desc *d = nullptr;
+  CUtensorMap *m = nullptr;
+  cudaError_t e = cudaMalloc(&d, cap * sizeof(Desc));
+  if (e == cudaSuccess) e = cudaMalloc(&m, 3 * cap * sizeof(CUtensorMap));
+  if (e == cudaSuccess && p.used) e = cudaMemcpy(d, p.descs, p.used * sizeof(Desc), cudaMemcpyDeviceToDevice);
+  if (e == cudaSuccess && p.used)
+    e = cudaMemcpy(m, p.maps, 3 * p.used * sizeof(CUtensorMap), cudaMemcpyDeviceToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    cudaFree(m);
+    return cuda_error(e, "server descriptor pool");
+  }
+  std::lock_guard<std::mutex> g(sv->mu);
+  if (p.descs) {
+    p.old.push_back(p.descs);
+    p.old.push_back(p.maps);
+  }
+  p.descs = d;
+  p.maps = m;
+  p.cap = cap;
+  return CGX_OK;
+}
+
+void pool_free(Pool &p) {
+  cudaFree(p.descs);
+  cudaFree(p.maps);
+  for (void *x : p.old) cudaFree(x);
+  p = Pool();
+}
+
 void slot_free(Slot &s) {
   if (s.stream) cudaStreamSynchronize(s.stream);
-  cudaFree(s.d_descs);
-  cudaFreeHost(s.h_descs);
   cudaFree(s.d_tmap);
   cudaFreeHost(s.h_tmap);
-  cudaFree(s.d_maps);
-  cudaFreeHost(s.h_maps);
   cudaFree(s.d_counter);
   cudaFree(s.d_status);
   if (s.done) cudaEventDestroy(s.done);
@@ -155,12 +197,13 @@ void slot_free(Slot &s) {
 }
 
 // Retire a slot whose kernel has finished.
-void retire(cgx_server *sv, Slot &s) {
+void retire(cgx_server *sv, int slot) {
+  Slot &s = sv->slots[slot];
   const double t = sv->now();
   std::lock_guard<std::mutex> g(sv->mu);
   for (int r : s.reqs) {
     sv->reqs[r].t_done = t;
-    sv->hier_busy[sv->ops[sv->reqs[r].op].hier] = 0;
+    sv->hier_in[slot][sv->ops[sv->reqs[r].op].hier] = 0;
   }
   sv->completed += (long long)s.reqs.size();
   s.reqs.clear();
@@ -168,24 +211,32 @@ void retire(cgx_server *sv, Slot &s) {
   sv->cv.notify_all();
 }
 
-// Batched mode: take the oldest pending request of every idle hierarchy
-// (in arrival order) that fits the slot, and launch them as one kernel.
-bool launch_batch(cgx_server *sv, Slot &s) {
+// Batched mode: take, in arrival order, the oldest pending request of every
+// hierarchy (one per hierarchy per launch) that fits the slot, and launch
+// them together.  A hierarchy whose previous request is in flight on the
+// other slot makes this slot's stream wait for that slot's completion.
+bool launch_batch(cgx_server *sv, int slot) {
+  Slot &s = sv->slots[slot];
+  const int other = 1 - slot;
   std::vector<int> take;
   std::vector<const OpTemplate *> tops; // the taken requests' operations
-  size_t ndesc = 0, ntiles = 0;
+  size_t ntiles = 0;
+  bool wait_other = false;
+  const Desc *pdescs;
+  const CUtensorMap *pmaps;
   {
     std::lock_guard<std::mutex> g(sv->mu);
-    std::vector<char> seen(sv->hier_busy.size(), 0);
+    pdescs = sv->pool.descs;
+    pmaps = sv->pool.maps;
+    std::vector<char> seen(sv->hier_in[0].size(), 0);
     for (auto it = sv->pending.begin(); it != sv->pending.end();) {
       const OpTemplate &op = sv->ops[sv->reqs[*it].op];
-      if (sv->hier_busy[op.hier] || seen[op.hier]) {
-        seen[op.hier] = 1; // keep this hierarchy's later requests behind it
+      if (seen[op.hier]) { // keep this hierarchy's later requests behind it
         ++it;
         continue;
       }
       seen[op.hier] = 1;
-      if (ndesc + op.descs.size() > s.desc_cap || ntiles + op.tiles > s.tile_cap) {
+      if (ntiles + (size_t)op.tiles > s.tile_cap) {
         if (take.empty()) { // larger than a slot (define_op rejects these): drop it
           sv->error = set_error(CGX_EINVAL, "request larger than a server slot");
           sv->reqs[*it].t_done = -1.0;
@@ -198,47 +249,40 @@ bool launch_batch(cgx_server *sv, Slot &s) {
       }
       take.push_back(*it);
       tops.push_back(&op);
-      ndesc += op.descs.size();
-      ntiles += op.tiles;
-      sv->hier_busy[op.hier] = 1;
+      ntiles += (size_t)op.tiles;
+      wait_other |= sv->hier_in[other][op.hier] != 0;
+      sv->hier_in[slot][op.hier] = 1;
       it = sv->pending.erase(it);
     }
   }
   if (take.empty()) return false;
-  // concatenate descriptors in pinned staging, and the tile maps segment
-  // by segment (prolongation tiles of all requests, then each streaming
-  // variant's), one persistent kernel per segment
-  size_t di = 0, ti = 0;
-  const double t = sv->now();
-  std::vector<int> base(take.size());
-  for (size_t q = 0; q < take.size(); ++q) {
-    const OpTemplate &op = *tops[q];
-    const size_t n = op.descs.size();
-    memcpy(s.h_descs + di, op.descs.data(), n * sizeof(Desc));
-    memcpy(s.h_maps + 3 * di, op.maps.data(), 3 * n * sizeof(CUtensorMap));
-    base[q] = (int)di;
-    di += n;
-    sv->reqs[take[q]].t_launch = t;
-  }
+  // the tile map, segment by segment (prolongation tiles of all requests,
+  // then each streaming variant's), one persistent kernel per segment; the
+  // entries already name pool descriptors
+  size_t ti = 0;
   long long seg[NSEG + 1];
   for (int g = 0; g < NSEG; ++g) {
     seg[g] = (long long)ti;
-    for (size_t q = 0; q < take.size(); ++q)
-      for (const int2 &e : tops[q]->seg_tiles[g]) s.h_tmap[ti++] = make_int2(e.x + base[q], e.y);
+    for (const OpTemplate *op : tops) {
+      const std::vector<int2> &v = op->seg_tiles[g];
+      if (!v.empty()) memcpy(s.h_tmap + ti, v.data(), v.size() * sizeof(int2));
+      ti += v.size();
+    }
   }
   seg[NSEG] = (long long)ti;
-  cudaError_t e = cudaMemcpyAsync(s.d_descs, s.h_descs, di * sizeof(Desc), cudaMemcpyHostToDevice, s.stream);
+  const double t = sv->now();
+  for (int r : take) sv->reqs[r].t_launch = t;
+  cudaError_t e = cudaSuccess;
+  if (wait_other) e = cudaStreamWaitEvent(s.stream, sv->slots[other].done, 0);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(s.d_tmap, s.h_tmap, ti * sizeof(int2), cudaMemcpyHostToDevice, s.stream);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(s.d_maps, s.h_maps, 3 * di * sizeof(CUtensorMap), cudaMemcpyHostToDevice, s.stream);
   int rc = e == cudaSuccess ? CGX_OK : cuda_error(e, "server slot upload");
   if (rc == CGX_OK && seg[NSEG] > 0) {
     e = cudaMemsetAsync(s.d_counter, 0, NSEG * sizeof(unsigned long long), s.stream);
     int need = 0;
-    rc = e == cudaSuccess ? launch_map_concurrent(sv->fp, s.d_descs, s.d_maps, s.d_tmap, seg, nullptr,
-                                                  s.d_counter, s.d_status, s.stream, s.side, s.ev,
-                                                  CONCURRENT_SIDE_MAX, &need)
+    rc = e == cudaSuccess ? launch_map_concurrent(sv->fp, pdescs, pmaps, s.d_tmap, seg, nullptr, s.d_counter,
+                                                  s.d_status, s.stream, s.side, s.ev, CONCURRENT_SIDE_MAX,
+                                                  &need)
                           : cuda_error(e, "cudaMemsetAsync");
   }
   if (rc) sv->error = rc;
@@ -286,14 +330,14 @@ void worker_loop(cgx_server *sv) {
     for (int i = 0; i < nslots; ++i) {
       Slot &s = sv->slots[i];
       if (s.busy && cudaEventQuery(s.done) == cudaSuccess) {
-        retire(sv, s);
+        retire(sv, i);
         progress = true;
       }
     }
     for (int i = 0; i < nslots; ++i) {
       Slot &s = sv->slots[i];
       if (!s.busy) {
-        bool l = sv->mode == CGX_SERVE_BATCHED ? launch_batch(sv, s) : launch_plain(sv, s);
+        bool l = sv->mode == CGX_SERVE_BATCHED ? launch_batch(sv, i) : launch_plain(sv, s);
         progress |= l;
       }
     }
@@ -357,9 +401,17 @@ int cgx_server_create(cgx_server **out, int mode, int64_t hbm_budget_bytes, int 
   sv->max_requests = (size_t)max_requests;
   sv->reqs.reserve(sv->max_requests);
   for (int i = 0; i < 2; ++i) {
-    int rc = slot_init(sv->slots[i], (size_t)max_pairs, (size_t)max_tiles);
+    int rc = slot_init(sv->slots[i], (size_t)max_tiles);
     if (rc) {
       for (int j = 0; j <= i; ++j) slot_free(sv->slots[j]);
+      delete sv;
+      return rc;
+    }
+  }
+  if (mode == CGX_SERVE_BATCHED) {
+    int rc = pool_reserve(sv, (size_t)max_pairs);
+    if (rc) {
+      for (int j = 0; j < 2; ++j) slot_free(sv->slots[j]);
       delete sv;
       return rc;
     }
@@ -376,6 +428,7 @@ int cgx_server_destroy(cgx_server *sv) {
     sv->worker.join();
   }
   for (int i = 0; i < 2; ++i) slot_free(sv->slots[i]);
+  pool_free(sv->pool);
   delete sv;
   return CGX_OK;
 }
@@ -409,22 +462,40 @@ int cgx_server_define_op(cgx_server *sv, int hier, const cgx_batch *pairs, int *
   op.hier = hier;
   op.descs.assign(d, d + n);
   op.ntiles.assign(nt, nt + n);
-  op.maps.resize(3 * (size_t)n);
+  std::vector<CUtensorMap> maps(3 * (size_t)n);
   for (int i = 0; i < n; ++i)
-    if (is_stencil(op.descs[i].kind) && !encode_tma_maps(op.descs[i], &op.maps[3 * (size_t)i]))
+    if (is_stencil(op.descs[i].kind) && !encode_tma_maps(op.descs[i], &maps[3 * (size_t)i]))
       op.descs[i].bx = 0;
   for (int i = 0; i < n; ++i) {
     op.tiles += nt[i];
     op.points += pts[i];
     op.bytes += byt[i];
-    std::vector<int2> &st = op.seg_tiles[segment_of(op.descs[i])];
-    for (int j = 0; j < nt[i]; ++j) st.push_back(make_int2(i, j));
   }
-  if (op.descs.size() > sv->slots[0].desc_cap || (size_t)op.tiles > sv->slots[0].tile_cap)
-    return set_error(CGX_EINVAL, "operation larger than a server slot");
+  if ((size_t)op.tiles > sv->slots[0].tile_cap) return set_error(CGX_EINVAL, "operation larger than a server slot");
+  // batched mode: the descriptors and tensor maps go into the device pool
+  // once (synchronous copies: the operation is usable when this returns),
+  // and the tiles are kept with pool indices
+  std::lock_guard<std::mutex> dg(sv->define_mu);
+  if (sv->mode == CGX_SERVE_BATCHED && n > 0) {
+    rc = pool_reserve(sv, sv->pool.used + (size_t)n);
+    if (rc) return rc;
+    const size_t base = sv->pool.used;
+    cudaError_t e = cudaMemcpy(sv->pool.descs + base, op.descs.data(), (size_t)n * sizeof(Desc),
+                               cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(sv->pool.maps + 3 * base, maps.data(), 3 * (size_t)n * sizeof(CUtensorMap),
+                     cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_error(e, "server operation upload");
+    for (int i = 0; i < n; ++i) {
+      std::vector<int2> &st = op.seg_tiles[segment_of(op.descs[i])];
+      for (int j = 0; j < nt[i]; ++j) st.push_back(make_int2((int)(base + (size_t)i), j));
+    }
+    sv->pool.used = base + (size_t)n;
+  }
   std::lock_guard<std::mutex> g(sv->mu); // the worker may be running
   sv->ops.push_back(std::move(op));
-  if ((int)sv->hier_busy.size() <= hier) sv->hier_busy.resize(hier + 1, 0);
+  for (int k = 0; k < 2; ++k)
+    if ((int)sv->hier_in[k].size() <= hier) sv->hier_in[k].resize(hier + 1, 0);
   *op_id = (int)sv->ops.size() - 1;
   return CGX_OK;
 }

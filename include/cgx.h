@@ -268,11 +268,17 @@ int cgx_graph_destroy(cgx_graph *g);
  * NO COUNTERPART IN THE REFERENCE (Carpet runs one hierarchy per job); the
  * operations served are the reference's (sync, boundary prolongation,
  * restriction of one level), each defined once from a cgx_batch holding its
- * box-pairs.  A worker thread continuously batches pending requests -- the
- * oldest of every hierarchy with nothing on the GPU -- into the persistent
- * kernel on two alternating launch slots; a hierarchy's requests run one
- * after another in arrival order.  CGX_SERVE_PLAIN serves one request at a
- * time through per-box launches (the baseline).  Hierarchies are admitted
+ * box-pairs; its descriptors and tensor maps are uploaded once into a
+ * device pool.  A worker thread continuously batches pending requests -- the
+ * oldest of every hierarchy, one per hierarchy per launch -- into the
+ * persistent kernels on two alternating launch slots; a hierarchy's requests
+ * run one after another in arrival order (a launch that takes a hierarchy
+ * still in flight on the other slot waits for that slot on the device, so
+ * the host prepares one slot while the GPU runs the other).
+ * CGX_SERVE_PLAIN serves one request at a time through per-box launches
+ * (the baseline).  max_pairs is the descriptor pool's initial capacity (it
+ * grows as operations are defined), max_tiles a launch's tile capacity.
+ * Hierarchies are admitted
  * against an HBM budget with cgx_server_admit/release; admission, release
  * and cgx_server_define_op are allowed while the worker runs, so that a
  * hierarchy admitted mid-stream is served from its first request on.  A
