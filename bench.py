@@ -84,6 +84,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--serve-seconds", type=float, default=1.0)
+    p.add_argument("--serve-config", type=int, default=None,
+                   help="tile configuration of the served prolongations (default SERVE_TILE_CONFIG)")
     p.add_argument("--no-tune", action="store_true", help="default tile configurations")
     p.add_argument("--tile-config", type=int, default=None,
                    help="pin every prolongation variant to this tile configuration instead of tuning")
@@ -291,7 +293,14 @@ def cpu_reference(h, ngf, seconds_per_step, steps, warmup):
 
 
 # ----------------------------------------------------------------- served
-def served(seconds: float, peak_gbs: float):
+# tile configuration of the served prolongations (the one the autotuner picks
+# for the step): on the served ensemble configurations 0, 2 and 1 measured
+# the same closed-loop rate (628-636 GB/s) and p50 0.42, 0.31 and 0.27 ms at
+# 1e5 requests/s; configuration 4 was slowest in a closed-loop sweep
+SERVE_TILE_CONFIG = 1
+
+
+def served(seconds: float, peak_gbs: float, tile_config: int = SERVE_TILE_CONFIG):
     """The served ensemble: 64 independent 3-level hierarchies (coarse sizes
     U{24..64} per axis, 4 grid functions x 3 timelevels, 2 components per
     level, each with a regrid-fill operation), admitted against a 150 GB HBM
@@ -305,7 +314,8 @@ def served(seconds: float, peak_gbs: float):
                                    poisson_trace)
     out = {"workload": "64 hierarchies x 3 vc levels, coarse U{24..64}^3, 4 GFs x 3 TLs, "
                        "order-5 prolongation + 3-TL time interpolation; Poisson stream "
-                       "sync/prolong/restrict 60/25/15", "budget_gb": 150, "rates": []}
+                       "sync/prolong/restrict 60/25/15", "budget_gb": 150,
+           "tile_config": tile_config, "rates": []}
     warm = Server(mode=SERVE_BATCHED)
     ens = Ensemble(warm, nhier=64, size_range=(24, 64), seed=42, regrid=True)
     plain = Server(mode=SERVE_PLAIN)
@@ -321,6 +331,8 @@ def served(seconds: float, peak_gbs: float):
 
     def run(mode, keys, arr):
         sv = Server(mode=mode)
+        if mode == SERVE_BATCHED:
+            sv.set_config(tile_config)
         op_ids = ens.define(sv)
         torch.cuda.synchronize()
         sv.replay(ops_for(op_ids, keys), arr)
@@ -771,7 +783,8 @@ def main():
 
     serve = None
     if rank == 0 and not args.no_serve:
-        serve = served(args.serve_seconds, peak)
+        serve = served(args.serve_seconds, peak,
+                       SERVE_TILE_CONFIG if args.serve_config is None else args.serve_config)
 
     batched_uneven = None
     if rank == 0 and not args.no_uneven:

@@ -1784,6 +1784,12 @@ int launch_tile_map(const Desc *d_descs, const CUtensorMap *d_maps, const int2 *
   return launch_map(fp, d_descs, d_maps, d_tmap, seg, nullptr, d_counter, d_status, s);
 }
 
+// A prolongation descriptor's tiles in TMA tile configuration `config`
+// (the tiling of a batch upload); returns the tile count, <= 0 if none.
+long long tile_prolongation(Desc &d, int config) {
+  return prolong_tiles(d, TMA_CFGS[config].pyc, TMA_CFGS[config].pz);
+}
+
 bool encode_tma_maps(const Desc &d, CUtensorMap maps[3]) {
   if (!is_stencil(d.kind) || d.bx == 0 || tma_variant(d) < 0) return false;
   // row and plane pitches must be multiples of 16 bytes

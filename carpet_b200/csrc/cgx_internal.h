@@ -60,6 +60,8 @@ constexpr int CONCURRENT_SIDE_MAX = NSEG;
 // true when the arrays can be staged by TMA (then maps[0 .. ntl-1] are
 // set), false otherwise.
 bool encode_tma_maps(const Desc &d, CUtensorMap maps[3]);
+// tiles of a prolongation descriptor in TMA tile configuration `config`
+long long tile_prolongation(Desc &d, int config);
 
 // One plain per-box launch (cgx.cu).
 int launch_one_pair(const Desc &d, int ntiles, int fp, int *status, cudaStream_t s);

@@ -109,6 +109,12 @@ struct cgx_server {
   std::deque<int> pending;
   Pool pool;             // grows under define_mu, read by the worker under mu
   std::mutex define_mu;  // serialises cgx_server_define_op
+  // the pool's uploads and copies, each waited for before the pool or the
+  // operation is published
+  cudaStream_t upload = nullptr;
+  // tile configuration per TMA prolongation variant (cgx_server_set_config),
+  // applied to operations defined afterwards
+  int tma_cfg[TV_COUNT] = {};
   std::mutex mu;
   std::condition_variable cv;
   std::thread worker;
@@ -155,9 +161,12 @@ int pool_reserve(cgx_server *sv, size_t need) {
   CUtensorMap *m = nullptr;
   cudaError_t e = cudaMalloc(&d, cap * sizeof(Desc));
   if (e == cudaSuccess) e = cudaMalloc(&m, 3 * cap * sizeof(CUtensorMap));
-  if (e == cudaSuccess && p.used) e = cudaMemcpy(d, p.descs, p.used * sizeof(Desc), cudaMemcpyDeviceToDevice);
   if (e == cudaSuccess && p.used)
-    e = cudaMemcpy(m, p.maps, 3 * p.used * sizeof(CUtensorMap), cudaMemcpyDeviceToDevice);
+    e = cudaMemcpyAsync(d, p.descs, p.used * sizeof(Desc), cudaMemcpyDeviceToDevice, sv->upload);
+  if (e == cudaSuccess && p.used)
+    e = cudaMemcpyAsync(m, p.maps, 3 * p.used * sizeof(CUtensorMap), cudaMemcpyDeviceToDevice, sv->upload);
+  // a device-to-device copy returns before it completes: wait for it
+  if (e == cudaSuccess) e = cudaStreamSynchronize(sv->upload);
   if (e != cudaSuccess) {
     cudaFree(d);
     cudaFree(m);
@@ -280,7 +289,7 @@ bool launch_batch(cgx_server *sv, int slot) {
   if (rc == CGX_OK && seg[NSEG] > 0) {
     e = cudaMemsetAsync(s.d_counter, 0, NSEG * sizeof(unsigned long long), s.stream);
     int need = 0;
-    rc = e == cudaSuccess ? launch_map_concurrent(sv->fp, pdescs, pmaps, s.d_tmap, seg, nullptr, s.d_counter,
+    rc = e == cudaSuccess ? launch_map_concurrent(sv->fp, pdescs, pmaps, s.d_tmap, seg, sv->tma_cfg, s.d_counter,
                                                   s.d_status, s.stream, s.side, s.ev, CONCURRENT_SIDE_MAX,
                                                   &need)
                           : cuda_error(e, "cudaMemsetAsync");
@@ -409,9 +418,12 @@ int cgx_server_create(cgx_server **out, int mode, int64_t hbm_budget_bytes, int 
     }
   }
   if (mode == CGX_SERVE_BATCHED) {
-    int rc = pool_reserve(sv, (size_t)max_pairs);
+    cudaError_t e = cudaStreamCreateWithFlags(&sv->upload, cudaStreamNonBlocking);
+    int rc = e == cudaSuccess ? pool_reserve(sv, (size_t)max_pairs) : cuda_error(e, "server upload stream");
     if (rc) {
       for (int j = 0; j < 2; ++j) slot_free(sv->slots[j]);
+      pool_free(sv->pool);
+      if (sv->upload) cudaStreamDestroy(sv->upload);
       delete sv;
       return rc;
     }
@@ -429,6 +441,7 @@ int cgx_server_destroy(cgx_server *sv) {
   }
   for (int i = 0; i < 2; ++i) slot_free(sv->slots[i]);
   pool_free(sv->pool);
+  if (sv->upload) cudaStreamDestroy(sv->upload);
   delete sv;
   return CGX_OK;
 }
@@ -462,12 +475,27 @@ int cgx_server_define_op(cgx_server *sv, int hier, const cgx_batch *pairs, int *
   op.hier = hier;
   op.descs.assign(d, d + n);
   op.ntiles.assign(nt, nt + n);
+  // the pool's copies: prolongations that TMA can stage are tiled in their
+  // variant's configuration and get tensor maps; the others run in the
+  // cp.async form on their default tiles
+  std::vector<Desc> pd(op.descs);
+  std::vector<long long> pnt(nt, nt + n);
   std::vector<CUtensorMap> maps(3 * (size_t)n);
-  for (int i = 0; i < n; ++i)
-    if (is_stencil(op.descs[i].kind) && !encode_tma_maps(op.descs[i], &maps[3 * (size_t)i]))
-      op.descs[i].bx = 0;
   for (int i = 0; i < n; ++i) {
-    op.tiles += nt[i];
+    if (!is_stencil(pd[i].kind)) continue;
+    const int v = tma_variant(pd[i]);
+    Desc t = pd[i];
+    long long tn = 0;
+    if (v >= 0) tn = tile_prolongation(t, sv->tma_cfg[v]);
+    if (v >= 0 && tn > 0 && tn < (1LL << 31) && encode_tma_maps(t, &maps[3 * (size_t)i])) {
+      pd[i] = t;
+      pnt[i] = tn;
+    } else {
+      pd[i].bx = 0;
+    }
+  }
+  for (int i = 0; i < n; ++i) {
+    op.tiles += sv->mode == CGX_SERVE_BATCHED ? pnt[i] : nt[i];
     op.points += pts[i];
     op.bytes += byt[i];
   }
@@ -480,15 +508,18 @@ int cgx_server_define_op(cgx_server *sv, int hier, const cgx_batch *pairs, int *
     rc = pool_reserve(sv, sv->pool.used + (size_t)n);
     if (rc) return rc;
     const size_t base = sv->pool.used;
-    cudaError_t e = cudaMemcpy(sv->pool.descs + base, op.descs.data(), (size_t)n * sizeof(Desc),
-                               cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpyAsync(sv->pool.descs + base, pd.data(), (size_t)n * sizeof(Desc),
+                                    cudaMemcpyHostToDevice, sv->upload);
     if (e == cudaSuccess)
-      e = cudaMemcpy(sv->pool.maps + 3 * base, maps.data(), 3 * (size_t)n * sizeof(CUtensorMap),
-                     cudaMemcpyHostToDevice);
+      e = cudaMemcpyAsync(sv->pool.maps + 3 * base, maps.data(), 3 * (size_t)n * sizeof(CUtensorMap),
+                          cudaMemcpyHostToDevice, sv->upload);
+    // from pageable memory a copy may return before its DMA lands: the
+    // operation is published only once the upload has completed
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sv->upload);
     if (e != cudaSuccess) return cuda_error(e, "server operation upload");
     for (int i = 0; i < n; ++i) {
-      std::vector<int2> &st = op.seg_tiles[segment_of(op.descs[i])];
-      for (int j = 0; j < nt[i]; ++j) st.push_back(make_int2((int)(base + (size_t)i), j));
+      std::vector<int2> &st = op.seg_tiles[segment_of(pd[i])];
+      for (long long j = 0; j < pnt[i]; ++j) st.push_back(make_int2((int)(base + (size_t)i), (int)j));
     }
     sv->pool.used = base + (size_t)n;
   }
@@ -497,6 +528,16 @@ int cgx_server_define_op(cgx_server *sv, int hier, const cgx_batch *pairs, int *
   for (int k = 0; k < 2; ++k)
     if ((int)sv->hier_in[k].size() <= hier) sv->hier_in[k].resize(hier + 1, 0);
   *op_id = (int)sv->ops.size() - 1;
+  return CGX_OK;
+}
+
+int cgx_server_set_config(cgx_server *sv, int variant, int config) {
+  if (!sv || variant < -1 || variant >= TV_COUNT || config < 0 || config >= TMA_NCFG)
+    return set_error(CGX_EINVAL, "server set_config: variant %d / configuration %d out of range", variant,
+                     config);
+  std::lock_guard<std::mutex> dg(sv->define_mu);
+  for (int v = 0; v < TV_COUNT; ++v)
+    if (variant < 0 || v == variant) sv->tma_cfg[v] = config;
   return CGX_OK;
 }
 

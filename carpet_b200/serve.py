@@ -47,6 +47,7 @@ lib.cgx_server_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int64, C.c
 for _f in ("cgx_server_destroy", "cgx_server_start", "cgx_server_drain"):
     getattr(lib, _f).argtypes = [C.c_void_p]
 lib.cgx_server_admit.argtypes = [C.c_void_p, C.c_int64]
+lib.cgx_server_set_config.argtypes = [C.c_void_p, C.c_int, C.c_int]
 lib.cgx_server_release.argtypes = [C.c_void_p, C.c_int64]
 lib.cgx_server_define_op.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int)]
 lib.cgx_server_submit.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int64)]
@@ -69,6 +70,11 @@ class Server:
             self.h = None
 
     __del__ = close
+
+    def set_config(self, config: int, variant: int = -1):
+        """tile configuration of the TMA prolongation variants (all: -1) for
+        operations defined from now on"""
+        check(lib.cgx_server_set_config(self.h, variant, config))
 
     def admit(self, nbytes: int) -> bool:
         rc = lib.cgx_server_admit(self.h, int(nbytes))

@@ -301,6 +301,9 @@ int cgx_server_destroy(cgx_server *s);
 int cgx_server_admit(cgx_server *s, int64_t bytes);   /* CGX_ENOMEM if over budget */
 int cgx_server_release(cgx_server *s, int64_t bytes);
 int cgx_server_define_op(cgx_server *s, int hier, const cgx_batch *pairs, int *op_id);
+/* tile configuration of a TMA prolongation variant (-1: all), as
+ * cgx_batch_set_config; applies to operations defined after the call */
+int cgx_server_set_config(cgx_server *s, int variant, int config);
 int cgx_server_start(cgx_server *s);
 int cgx_server_submit(cgx_server *s, int op_id, int64_t *request_id);
 /* submit op_ids[i] at arrival_s[i] seconds after the call (a load replay) */

@@ -38,15 +38,23 @@ def _equal(xs, ys):
                                       for a, b in zip(xs, ys))
 
 
-def test_batched_stream_equals_requests_alone(cgx):
+@pytest.mark.parametrize("config,burst", [(0, False), (2, False), (0, True), (2, True)])
+def test_batched_stream_equals_requests_alone(cgx, config, burst):
+    """a Poisson stream, or the same requests submitted at once (every
+    launch then takes the next request of hierarchies still in flight on the
+    other slot, ordered on the device by the slots' completion events), in
+    two tile configurations"""
     from carpet_b200.serve import (SERVE_BATCHED, SERVE_PLAIN, Ensemble, Server, ops_for,
                                    poisson_trace)
     cgx.set_fp_mode(False)
     batched = Server(mode=SERVE_BATCHED)
+    batched.set_config(config)
     plain = Server(mode=SERVE_PLAIN)
     ens = Ensemble(batched, nhier=8, size_range=(24, 40), seed=11, regrid=True)
     plain_ops = ens.define(plain)
     keys, arr = poisson_trace(ens, rate=1e5, n=300, seed=3, mix=(0.55, 0.25, 0.15, 0.05))
+    if burst:
+        arr = [0.0] * len(keys)
     init = ens.snapshot()
     batched.replay(ops_for(ens.ops, keys), arr)
     batched.drain()
