@@ -7,16 +7,16 @@
 // cgx_batch.  An operation's descriptors and tensor maps are uploaded once,
 // into a device pool that every launch reads, and its tiles are kept as
 // (pool descriptor, tile) entries by segment; a launch only concatenates
-// those entries into one tile map.  The worker thread keeps two launch
+// those entries into one tile map.  The worker thread keeps several launch
 // slots.  Whenever a slot is free it takes, in arrival order, the oldest
 // pending request of every hierarchy (one request per hierarchy per launch)
 // and launches the persistent kernels on that slot's stream.  A hierarchy
-// whose previous request is still in flight on the other slot may be taken:
-// the slot's stream then waits for the other slot's completion event before
-// its kernels, so each hierarchy sees its requests applied one after another
-// in arrival order -- the results are those of running them alone
-// (tests/test_gpu_serving.py) -- while the host prepares one slot as the
-// device runs the other.
+// whose previous request is still in flight on another slot may be taken:
+// the slot's stream then waits for that slot's completion event before its
+// kernels, so each hierarchy sees its requests applied one after another in
+// arrival order -- the results are those of running them alone
+// (tests/test_gpu_serving.py) -- while the host prepares the next launches
+// as the device runs the earlier ones.
 //
 // The plain mode serves the same stream through the per-box drop-in: one
 // request at a time, one kernel launch per box-pair.
@@ -50,6 +50,11 @@ using namespace cgx;
 namespace {
 
 using clk = std::chrono::steady_clock;
+
+// launch slots of the batched mode: with several, the host prepares the next
+// launches while the device runs earlier ones (a launch that takes a
+// hierarchy in flight on another slot waits for that slot on the device)
+constexpr int SERVER_SLOTS = 4;
 
 struct OpTemplate {
   int hier;
@@ -104,8 +109,9 @@ struct cgx_server {
   std::deque<OpTemplate> ops;
   std::vector<Request> reqs; // reserved at creation: never reallocated
   size_t max_requests = 0;
-  // per hierarchy: whether a request of it is in flight on slot 0 / slot 1
-  std::vector<unsigned char> hier_in[2];
+  // per hierarchy: the slot of its latest launched request while that is
+  // in flight, else -1
+  std::vector<signed char> hier_last;
   std::deque<int> pending;
   Pool pool;             // grows under define_mu, read by the worker under mu
   std::mutex define_mu;  // serialises cgx_server_define_op
@@ -121,7 +127,7 @@ struct cgx_server {
   std::atomic<bool> stop{false};
   std::atomic<long long> completed{0};
   long long submitted = 0;
-  Slot slots[2];
+  Slot slots[SERVER_SLOTS];
   clk::time_point epoch = clk::now();
   long long launches = 0, batched_requests = 0;
   int error = CGX_OK;
@@ -212,7 +218,8 @@ void retire(cgx_server *sv, int slot) {
   std::lock_guard<std::mutex> g(sv->mu);
   for (int r : s.reqs) {
     sv->reqs[r].t_done = t;
-    sv->hier_in[slot][sv->ops[sv->reqs[r].op].hier] = 0;
+    signed char &last = sv->hier_last[sv->ops[sv->reqs[r].op].hier];
+    if (last == slot) last = -1; // no later launch took this hierarchy
   }
   sv->completed += (long long)s.reqs.size();
   s.reqs.clear();
@@ -222,22 +229,21 @@ void retire(cgx_server *sv, int slot) {
 
 // Batched mode: take, in arrival order, the oldest pending request of every
 // hierarchy (one per hierarchy per launch) that fits the slot, and launch
-// them together.  A hierarchy whose previous request is in flight on the
-// other slot makes this slot's stream wait for that slot's completion.
+// them together.  A hierarchy whose previous request is in flight on another
+// slot makes this slot's stream wait for that slot's completion.
 bool launch_batch(cgx_server *sv, int slot) {
   Slot &s = sv->slots[slot];
-  const int other = 1 - slot;
   std::vector<int> take;
   std::vector<const OpTemplate *> tops; // the taken requests' operations
   size_t ntiles = 0;
-  bool wait_other = false;
+  bool wait_for[SERVER_SLOTS] = {};
   const Desc *pdescs;
   const CUtensorMap *pmaps;
   {
     std::lock_guard<std::mutex> g(sv->mu);
     pdescs = sv->pool.descs;
     pmaps = sv->pool.maps;
-    std::vector<char> seen(sv->hier_in[0].size(), 0);
+    std::vector<char> seen(sv->hier_last.size(), 0);
     for (auto it = sv->pending.begin(); it != sv->pending.end();) {
       const OpTemplate &op = sv->ops[sv->reqs[*it].op];
       if (seen[op.hier]) { // keep this hierarchy's later requests behind it
@@ -259,8 +265,9 @@ bool launch_batch(cgx_server *sv, int slot) {
       take.push_back(*it);
       tops.push_back(&op);
       ntiles += (size_t)op.tiles;
-      wait_other |= sv->hier_in[other][op.hier] != 0;
-      sv->hier_in[slot][op.hier] = 1;
+      signed char &last = sv->hier_last[op.hier];
+      if (last >= 0) wait_for[last] = true;
+      last = (signed char)slot;
       it = sv->pending.erase(it);
     }
   }
@@ -282,7 +289,8 @@ bool launch_batch(cgx_server *sv, int slot) {
   const double t = sv->now();
   for (int r : take) sv->reqs[r].t_launch = t;
   cudaError_t e = cudaSuccess;
-  if (wait_other) e = cudaStreamWaitEvent(s.stream, sv->slots[other].done, 0);
+  for (int k = 0; k < SERVER_SLOTS && e == cudaSuccess; ++k)
+    if (wait_for[k]) e = cudaStreamWaitEvent(s.stream, sv->slots[k].done, 0);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(s.d_tmap, s.h_tmap, ti * sizeof(int2), cudaMemcpyHostToDevice, s.stream);
   int rc = e == cudaSuccess ? CGX_OK : cuda_error(e, "server slot upload");
@@ -333,7 +341,7 @@ bool launch_plain(cgx_server *sv, Slot &s) {
 }
 
 void worker_loop(cgx_server *sv) {
-  const int nslots = sv->mode == CGX_SERVE_BATCHED ? 2 : 1;
+  const int nslots = sv->mode == CGX_SERVE_BATCHED ? SERVER_SLOTS : 1;
   for (;;) {
     bool progress = false;
     for (int i = 0; i < nslots; ++i) {
@@ -409,7 +417,8 @@ int cgx_server_create(cgx_server **out, int mode, int64_t hbm_budget_bytes, int 
   sv->fp = current_fp_mode();
   sv->max_requests = (size_t)max_requests;
   sv->reqs.reserve(sv->max_requests);
-  for (int i = 0; i < 2; ++i) {
+  const int nslots = mode == CGX_SERVE_BATCHED ? SERVER_SLOTS : 1;
+  for (int i = 0; i < nslots; ++i) {
     int rc = slot_init(sv->slots[i], (size_t)max_tiles);
     if (rc) {
       for (int j = 0; j <= i; ++j) slot_free(sv->slots[j]);
@@ -421,7 +430,7 @@ int cgx_server_create(cgx_server **out, int mode, int64_t hbm_budget_bytes, int 
     cudaError_t e = cudaStreamCreateWithFlags(&sv->upload, cudaStreamNonBlocking);
     int rc = e == cudaSuccess ? pool_reserve(sv, (size_t)max_pairs) : cuda_error(e, "server upload stream");
     if (rc) {
-      for (int j = 0; j < 2; ++j) slot_free(sv->slots[j]);
+      for (int j = 0; j < nslots; ++j) slot_free(sv->slots[j]);
       pool_free(sv->pool);
       if (sv->upload) cudaStreamDestroy(sv->upload);
       delete sv;
@@ -439,7 +448,7 @@ int cgx_server_destroy(cgx_server *sv) {
     sv->cv.notify_all();
     sv->worker.join();
   }
-  for (int i = 0; i < 2; ++i) slot_free(sv->slots[i]);
+  for (int i = 0; i < SERVER_SLOTS; ++i) slot_free(sv->slots[i]);
   pool_free(sv->pool);
   if (sv->upload) cudaStreamDestroy(sv->upload);
   delete sv;
@@ -525,8 +534,7 @@ int cgx_server_define_op(cgx_server *sv, int hier, const cgx_batch *pairs, int *
   }
   std::lock_guard<std::mutex> g(sv->mu); // the worker may be running
   sv->ops.push_back(std::move(op));
-  for (int k = 0; k < 2; ++k)
-    if ((int)sv->hier_in[k].size() <= hier) sv->hier_in[k].resize(hier + 1, 0);
+  if ((int)sv->hier_last.size() <= hier) sv->hier_last.resize(hier + 1, -1);
   *op_id = (int)sv->ops.size() - 1;
   return CGX_OK;
 }

@@ -271,10 +271,10 @@ int cgx_graph_destroy(cgx_graph *g);
  * box-pairs; its descriptors and tensor maps are uploaded once into a
  * device pool.  A worker thread continuously batches pending requests -- the
  * oldest of every hierarchy, one per hierarchy per launch -- into the
- * persistent kernels on two alternating launch slots; a hierarchy's requests
- * run one after another in arrival order (a launch that takes a hierarchy
- * still in flight on the other slot waits for that slot on the device, so
- * the host prepares one slot while the GPU runs the other).
+ * persistent kernels on four launch slots; a hierarchy's requests run one
+ * after another in arrival order (a launch that takes a hierarchy still in
+ * flight on another slot waits for that slot on the device, so the host
+ * prepares the next launches while the GPU runs the earlier ones).
  * CGX_SERVE_PLAIN serves one request at a time through per-box launches
  * (the baseline).  max_pairs is the descriptor pool's initial capacity (it
  * grows as operations are defined), max_tiles a launch's tile capacity.
