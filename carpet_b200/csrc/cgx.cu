@@ -128,6 +128,40 @@ long long prolong_tiles(Desc &d, int pycmax, int pz) {
   return tot;
 }
 
+// Prolongation tiles of the TMA kernels in tile configuration `config`: as
+// prolong_tiles, with as many coarse rows per tile as the configuration's
+// threads (one owner per fine x and coarse row), staged box, x-pass rows and
+// x items allow for the tile's width (the limits of cgx_tma.cuh): in a
+// 128-thread configuration a tile of 16 fine x takes 8 rows, one of 12 takes
+// 10 and one of 6 takes 11 (the x-pass rows' limit).
+long long prolong_tiles_tma(Desc &d, int config) {
+  const TmaCfg &c = TMA_CFGS[config];
+  const Win w = family_window(d.kind, d.order);
+  const int W = std::max(w.hi0, w.hi1) - std::min(w.lo0, w.lo1);
+  const int ntx = (d.n[0] + PTXMAX - 1) / PTXMAX;
+  const int ptx = (d.n[0] + ntx - 1) / ntx;
+  const int bx = ((ptx + 2) / 2 + W + 2) & ~1;
+  const int xr = TMA_XR, nbx = ptx / 2 + 1, ntl = std::max(1, (int)d.ntl);
+  int rmax = c.nt / ptx;
+  rmax = std::min(rmax, tma_tls(W, c.pyc) / bx - W);
+  rmax = std::min(rmax, (tma_xbuf(W, c.pyc, ntl) / xr - 1) / ntl - W);
+  rmax = std::min(rmax, tma_items(W, c.pyc) / nbx - W);
+  if (rmax < 1) return -1;
+  const int nty = (d.n[1] + 2 * rmax - 2) / (2 * rmax - 1);
+  const int pty = (d.n[1] + nty - 1) / nty;
+  const int ptyc = std::min(rmax, (pty + 2) / 2);
+  d.ptx = (unsigned char)ptx;
+  d.ptyc = (unsigned char)ptyc;
+  d.bx = (unsigned char)bx;
+  d.by = (unsigned char)(ptyc + W);
+  d.tiles[0] = (d.n[0] + ptx - 1) / ptx;
+  d.tiles[1] = (d.n[1] + 2 * ptyc - 2) / (2 * ptyc - 1);
+  d.tiles[2] = (d.n[2] + c.pz - 1) / c.pz;
+  long long tot = 1;
+  for (int k = 0; k < 3; ++k) tot *= d.tiles[k];
+  return tot;
+}
+
 // Tiles of a descriptor.  Prolongation: the default configuration of
 // prolong_tiles (PTYCMAX rows, PTZ fine z).  Copy and restriction: STILE
 // consecutive points of the flattened region.
@@ -1039,10 +1073,7 @@ int cgx_batch_upload(cgx_batch *b, void *stream) {
     const int v = tma_variant(dq[i]);
     Desc t = dq[i];
     long long nt = 0;
-    if (v >= 0) {
-      const TmaCfg &c = TMA_CFGS[b->tma_cfg[v]];
-      nt = prolong_tiles(t, c.pyc, c.pz);
-    }
+    if (v >= 0) nt = prolong_tiles_tma(t, b->tma_cfg[v]);
     if (v >= 0 && nt > 0 && nt < (1LL << 31) && encode_tma_maps(t, &em[3 * (size_t)i])) {
       dq[i] = t;
       ntq[i] = nt;
@@ -1421,7 +1452,6 @@ int cgx_chain_upload(cgx_chain *c, void *stream) {
   if (!c) return fail(CGX_EINVAL, "null chain");
   cudaStream_t s = (cudaStream_t)stream;
   constexpr int CFG = 1; // the chain kernel's prolongation tile configuration
-  const TmaCfg &cfg = TMA_CFGS[CFG];
   std::vector<Desc> hd;
   std::vector<CUtensorMap> hm;
   std::vector<ChainTile> ht;
@@ -1456,7 +1486,7 @@ int cgx_chain_upload(cgx_chain *c, void *stream) {
           if (order >= 0 && d.order != order)
             return fail(CGX_EUNSUPPORTED, "chain: prolongation orders %d and %d mixed", order, d.order);
           order = d.order;
-          nt = prolong_tiles(d, cfg.pyc, cfg.pz);
+          nt = prolong_tiles_tma(d, CFG);
           if (nt <= 0 || nt >= (1LL << 31) || !encode_tma_maps(d, maps))
             return fail(CGX_EUNSUPPORTED,
                         "chain: batch %zu pair %d: the source arrays cannot be staged by TMA "
@@ -1787,7 +1817,7 @@ int launch_tile_map(const Desc *d_descs, const CUtensorMap *d_maps, const int2 *
 // A prolongation descriptor's tiles in TMA tile configuration `config`
 // (the tiling of a batch upload); returns the tile count, <= 0 if none.
 long long tile_prolongation(Desc &d, int config) {
-  return prolong_tiles(d, TMA_CFGS[config].pyc, TMA_CFGS[config].pz);
+  return prolong_tiles_tma(d, config);
 }
 
 bool encode_tma_maps(const Desc &d, CUtensorMap maps[3]) {

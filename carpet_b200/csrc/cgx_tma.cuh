@@ -37,25 +37,38 @@ constexpr TmaCfg TMA_CFGS[] = {
 constexpr int TMA_NCFG = 5;
 constexpr int TMA_NB_MAX = 5; // ring slots, at most (pd + 2)
 
+// Shared-memory geometry of a tile configuration with PYC coarse rows for a
+// stencil window of width W (host and device).  A tile of ptx fine x uses
+// ptx * ptyc owner threads; ptyc may exceed PYC when ptx < 16, as far as the
+// staged box, the x-pass rows and the x items fit (tma_rows_max, host).
+//   coarse box      bx = (ptx + 2) / 2 bases + the window + one point of
+//                   even-alignment shift, rounded up to even; by = ptyc + W
+//                   rows; bx * by <= tma_tls doubles per (slot, timelevel)
+//   x-pass rows     ntl * by rows of pitch TMA_XR (two fine points per coarse
+//                   base: at most ptx + 2 <= 18), + one spare row for masked
+//                   x items; a half-warp of the y pass reads one row when
+//                   ptx = 16, at most three short rows otherwise
+//   x items         (timelevel, coarse row, coarse base), at most
+//                   ntl * tma_items per tile
+constexpr int TMA_EXTRA_ROWS = 3; // rows staged beyond PYC + W (for ptx < 16)
+__host__ __device__ constexpr int tma_bxmax(int W) { return ((PTXMAX + 2) / 2 + W + 2) & ~1; }
+__host__ __device__ constexpr int tma_bymax(int W, int pyc) { return pyc + W + TMA_EXTRA_ROWS; }
+__host__ __device__ constexpr int tma_tls(int W, int pyc) { return (tma_bxmax(W) * tma_bymax(W, pyc) + 15) / 16 * 16; }
+constexpr int TMA_XR = PTXMAX + 2; // even: 16-byte rows
+__host__ __device__ constexpr int tma_xbuf(int W, int pyc, int ntl) { return (ntl * tma_bymax(W, pyc) + 1) * TMA_XR; }
+__host__ __device__ constexpr int tma_items(int W, int pyc) { return (pyc + W) * ((PTXMAX + 2) / 2); }
+
 template <class F, int PYC = PTYCMAX> struct TGeom {
   static constexpr int W = F::HI - F::LO;
-  // box: up to (PTXMAX + 2) / 2 coarse bases + the window + one point of
-  // even-alignment shift, rounded up to even; by = ptyc + W rows
-  static constexpr int BXMAX = ((PTXMAX + 2) / 2 + W + 2) & ~1;
-  static constexpr int BYMAX = PYC + W;
-  static constexpr int TLS = (BXMAX * BYMAX + 15) / 16 * 16; // doubles per (slot, timelevel)
-  static constexpr int CY = BYMAX;                            // x-pass rows per timelevel
-  // x-pass row pitch: two fine points per coarse base; the y pass's lane
-  // (row i / 16, column i % 16) then reads word i modulo 16, so a
-  // half-warp's 8-byte loads meet no bank conflict
-  static constexpr int XR = 2 * PTXMAX;
+  static constexpr int TLS = tma_tls(W, PYC); // doubles per (slot, timelevel)
+  static constexpr int ITEMS = tma_items(W, PYC);
   static constexpr int Q = W + 1;
 };
 template <class F, int NTL, int PYC = PTYCMAX, int NB = 5> struct TSmem {
   using G = TGeom<F, PYC>;
   static constexpr int coarse = NB * NTL * G::TLS;
-  static constexpr int xbuf = (NTL * G::CY + 1) * G::XR; // + one row for masked x items
-  static constexpr int total = coarse + 2 * xbuf;        // doubles
+  static constexpr int xbuf = tma_xbuf(G::W, PYC, NTL);
+  static constexpr int total = coarse + 2 * xbuf; // doubles
 };
 
 // The TMA kernels' variants: family (VC 1/3/5, CC 0-5, ENO) x time
@@ -143,7 +156,9 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
   const int tid = threadIdx.x;
   const int ptx = d.ptx, ptyc = d.ptyc, pty = 2 * ptyc - 1;
   const int BX = d.bx, BY = d.by;
-  constexpr int XR = G::XR;
+  // x-pass rows: BY per timelevel, pitch XR
+  constexpr int XR = TMA_XR;
+  const int CY = BY;
 
   const int tx = tile % d.tiles[0], rr = tile / d.tiles[0];
   const int ty = rr % d.tiles[1], tz = rr / d.tiles[1];
@@ -178,7 +193,7 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
   };
 
   // --- x items: (timelevel, row, base) spread over the CTA
-  constexpr int IT = (NTL * G::CY * ((PTXMAX + 2) / 2) + NT - 1) / NT; // nbx <= 9
+  constexpr int IT = (NTL * G::ITEMS + NT - 1) / NT; // ncy * nbx <= ITEMS
   const int per_t = ncy * nbx, count = NTL * per_t;
   int xsrc[IT], xdst[IT];
 #pragma unroll
@@ -188,10 +203,10 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
       const int t = it / per_t, rem = it - t * per_t;
       const int r = rem / nbx, b = rem - r * nbx;
       xsrc[k] = t * G::TLS + r * BX + xs + b; // window element j of base b at xsrc + j - LO
-      xdst[k] = (t * G::CY + r) * XR + 2 * b;
+      xdst[k] = (t * CY + r) * XR + 2 * b;
     } else {
       xsrc[k] = 0;
-      xdst[k] = NTL * G::CY * XR; // the spare row
+      xdst[k] = NTL * CY * XR; // the spare row
     }
   }
   auto xpass = [&](int slot, double *__restrict__ xr) {
@@ -210,11 +225,13 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
     }
   };
 
-  // --- y/z owner: thread = (fine x, coarse y row) = (tid % 16, tid / 16)
-  static_assert(PTXMAX == 16 && NT == 16 * PYC, "y/z thread layout");
-  const int my_fx = tid & 15, my_cyr = tid >> 4;
-  const bool tact = my_fx < ptx && my_cyr < ptyc;
-  const bool wact = 2 * (tid >> 5) < ptyc; // warp holds an owner
+  // --- y/z owner: thread = (fine x, coarse y row) = (tid % ptx, tid / ptx);
+  // threads past the ptx * ptyc owners address row ptyc - 1 and store nothing
+  static_assert(PTXMAX == 16 && NT == 16 * PYC, "y/z thread layout of a full-width tile");
+  const int my_fx = tid % ptx, my_cyr_all = tid / ptx;
+  const bool tact = my_cyr_all < ptyc;
+  const int my_cyr = tact ? my_cyr_all : ptyc - 1;
+  const bool wact = (tid & ~31) / ptx < ptyc; // warp holds an owner
   const int my_cy = (sy0 >> 1) + my_cyr;
   const int ys0 = 2 * my_cy;
   const bool xin = tact && my_fx < nfx;
@@ -241,7 +258,7 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
     if (!wact) return; // warp-uniform
 #pragma unroll
     for (int t = 0; t < NTL; ++t) {
-      const double *col = xr + t * G::CY * XR + ycol;
+      const double *col = xr + t * CY * XR + ycol;
       auto get = [&](int m) { return col[m * XR]; };
       yq[t][0][U] = F::template next<FMA>(0, get);
       yq[t][1][U] = F::template next<FMA>(1, get);
