@@ -17,7 +17,12 @@
  *   fma == 1  every multiply-add contracted the way GCC contracts the same
  *             expressions under -mfma -ffp-contract=fast.
  * Both are pinned bit-for-bit against the reference's own operators,
- * compiled unchanged (oracle/Makefile -> oracle/_ref/), by tests/.
+ * compiled unchanged (oracle/Makefile -> oracle/_ref/), by tests/ -- except
+ * the vertex-centred ENO of prolongate_3d_real8_eno.F90, which is Fortran:
+ * with no Fortran compiler here its parity is unpinned by a compiled
+ * reference, and tests/test_eno_restatement.py checks it instead against a
+ * second, independent restatement of the Fortran source and against the
+ * properties the routine guarantees.
  *
  * Boxes are int[9] = {lower[3], upper[3], stride[3]} (inclusive bounds), the
  * layout CarpetLib passes to its Fortran operators (data.cc:212-214).
