@@ -366,3 +366,44 @@ def poisson_trace(ens: Ensemble, rate: float, n: int, seed=0, mix=(0.60, 0.25, 0
 
 def ops_for(op_ids: Dict[Tuple[int, str, int], int], keys):
     return [op_ids[k] for k in keys]
+
+
+def main(argv=None):
+    """``python -m carpet_b200.serve``: drive one served ensemble (64
+    hierarchies as in the benchmark) with a Poisson stream, or with every
+    request submitted at once (``--rate 0``: the closed-loop saturation
+    point), and print the server's report as one JSON line"""
+    import argparse
+    import json
+
+    import torch
+    p = argparse.ArgumentParser(prog="python -m carpet_b200.serve")
+    p.add_argument("--requests", type=int, default=20000)
+    p.add_argument("--rate", type=float, default=0.0, help="requests/s; 0: all at once")
+    p.add_argument("--plain", action="store_true", help="the plain per-box server")
+    p.add_argument("--tile-config", type=int, default=1)
+    p.add_argument("--hierarchies", type=int, default=64)
+    a = p.parse_args(argv)
+    warm = Server(mode=SERVE_BATCHED)
+    ens = Ensemble(warm, nhier=a.hierarchies, size_range=(24, 64), seed=42, regrid=True)
+    wk, wa = poisson_trace(ens, 1e4, 200, seed=1)  # warm-up: module loading, kernel attributes
+    warm.replay(ops_for(ens.ops, wk), wa)
+    warm.drain()
+    sv = Server(mode=SERVE_PLAIN if a.plain else SERVE_BATCHED)
+    if not a.plain:
+        sv.set_config(a.tile_config)
+    op_ids = ens.define(sv)
+    torch.cuda.synchronize()
+    keys, arr = poisson_trace(ens, a.rate if a.rate > 0 else 1e5, a.requests, seed=99)
+    sv.replay(ops_for(op_ids, keys), arr if a.rate > 0 else [0.0] * len(keys))
+    sv.drain()
+    r = sv.report()
+    r["gbs"] = r["bytes_per_s"] / 1e9
+    r["us_per_launch"] = 1e6 * r["makespan_s"] / max(1, r["launches"])
+    print(json.dumps({k: (round(v, 6) if isinstance(v, float) else v) for k, v in r.items()}))
+    sv.close()
+    warm.close()
+
+
+if __name__ == "__main__":
+    main()
