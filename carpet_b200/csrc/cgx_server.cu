@@ -162,7 +162,7 @@ int slot_init(Slot &s, size_t tile_cap) {
 int pool_reserve(cgx_server *sv, size_t need) {
   Pool &p = sv->pool;
   if (need <= p.cap) return CGX_OK;
-  size_t cap = std::max<size_t>(p.cap ? 2 * p.cap : 4096, need);
+  const size_t cap = p.cap ? std::max<size_t>(2 * p.cap, need) : need;
   Desc *d = nullptr;
   CUtensorMap *m = nullptr;
   cudaError_t e = cudaMalloc(&d, cap * sizeof(Desc));

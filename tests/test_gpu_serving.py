@@ -38,16 +38,18 @@ def _equal(xs, ys):
                                       for a, b in zip(xs, ys))
 
 
-@pytest.mark.parametrize("config,burst", [(0, False), (2, False), (0, True), (2, True)])
-def test_batched_stream_equals_requests_alone(cgx, config, burst):
+@pytest.mark.parametrize("config,burst,pool", [(0, False, 65536), (2, False, 65536), (0, True, 65536),
+                                               (2, True, 65536), (1, True, 16)])
+def test_batched_stream_equals_requests_alone(cgx, config, burst, pool):
     """a Poisson stream, or the same requests submitted at once (every
-    launch then takes the next request of hierarchies still in flight on the
-    other slot, ordered on the device by the slots' completion events), in
-    two tile configurations"""
+    launch then takes the next request of hierarchies still in flight on
+    another slot, ordered on the device by the slots' completion events), in
+    several tile configurations; with a descriptor pool of 16 entries at
+    first, which the operations' definitions grow many times over"""
     from carpet_b200.serve import (SERVE_BATCHED, SERVE_PLAIN, Ensemble, Server, ops_for,
                                    poisson_trace)
     cgx.set_fp_mode(False)
-    batched = Server(mode=SERVE_BATCHED)
+    batched = Server(mode=SERVE_BATCHED, max_pairs=pool)
     batched.set_config(config)
     plain = Server(mode=SERVE_PLAIN)
     ens = Ensemble(batched, nhier=8, size_range=(24, 40), seed=11, regrid=True)
@@ -135,7 +137,9 @@ def test_admission_while_serving(cgx):
     cgx.set_fp_mode(False)
     h = nested(3, (25, 25, 25), parts=(2, 1, 1), ghost=3, buffer=3, order=5)
     one = storage_bytes(h, 4, 3)
-    sv = Server(mode=SERVE_BATCHED, hbm_budget=int(3.5 * one))
+    # a small descriptor pool: the operations defined mid-stream grow it while
+    # the worker launches from it
+    sv = Server(mode=SERVE_BATCHED, hbm_budget=int(3.5 * one), max_pairs=64)
     plain = Server(mode=SERVE_PLAIN)
     ens = Ensemble(sv, nhier=5, size_range=(24, 24), seed=7)
     assert len(ens.members) == 3 and ens.deferred == 2
@@ -148,10 +152,17 @@ def test_admission_while_serving(cgx):
     m = new[0]
     init = [p.clone() for p in ens.state(m)]
     rng = np.random.default_rng(3)
+    # work queued on the other hierarchies, then more definitions: the pool
+    # grows (copied into a larger allocation) while those launches read it
+    busy = [request_key(ens, 1 + i % 2, int(rng.integers(0, 3)), rng) for i in range(200)]
+    sv.replay(ops_for(ens.ops, busy), [0.0] * len(busy))
+    for _ in range(3):
+        ops_now = ens.define(sv)
+    sv.drain()
     mine = [request_key(ens, m, int(rng.integers(0, 3)), rng) for _ in range(20)]
     others = [request_key(ens, 1 + i % 2, int(rng.integers(0, 3)), rng) for i in range(20)]
     stream = [k for pair in zip(mine, others) for k in pair]
-    sv.replay(ops_for(ens.ops, stream), [1e-5 * i for i in range(len(stream))])
+    sv.replay(ops_for(ops_now, stream), [1e-5 * i for i in range(len(stream))])
     sv.drain()
     got = [p.clone() for p in ens.state(m)]
     for p, q in zip(ens.state(m), init):
