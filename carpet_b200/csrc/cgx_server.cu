@@ -39,6 +39,7 @@
 #include <cstring>
 #include <deque>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -79,7 +80,10 @@ struct Slot {
   cudaEvent_t ev[CONCURRENT_SIDE_MAX + 1] = {};
   int2 *d_tmap = nullptr, *h_tmap = nullptr;
   unsigned long long *d_counter = nullptr;
-  int *d_status = nullptr;
+  // the launch's device status (a bounded wait that gave up: CGX_EDEVICE),
+  // zeroed before the kernels and copied to pinned memory after them; the
+  // worker reads it when it retires the slot
+  int *d_status = nullptr, *h_status = nullptr;
   size_t tile_cap = 0;
   bool busy = false;
   std::vector<int> reqs;
@@ -130,12 +134,26 @@ struct cgx_server {
   Slot slots[SERVER_SLOTS];
   clk::time_point epoch = clk::now();
   long long launches = 0, batched_requests = 0;
+  // the worker's first error and its message, which drain() reports in the
+  // caller's thread (under err_mu; taken after mu where both are held)
   int error = CGX_OK;
+  std::string error_msg;
+  std::mutex err_mu;
 
   double now() const { return std::chrono::duration<double>(clk::now() - epoch).count(); }
 };
 
 namespace {
+
+// Records the worker's first error: a status code whose message the calling
+// thread has just set (cgx_last_error is per thread).
+void note_error(cgx_server *sv, int rc) {
+  if (rc == CGX_OK) return;
+  std::lock_guard<std::mutex> g(sv->err_mu);
+  if (sv->error != CGX_OK) return;
+  sv->error = rc;
+  sv->error_msg = cgx_last_error();
+}
 
 int slot_init(Slot &s, size_t tile_cap) {
   cudaError_t e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
@@ -148,6 +166,8 @@ int slot_init(Slot &s, size_t tile_cap) {
   if (e == cudaSuccess) e = cudaMemset(s.d_counter, 0, 2 * NSEG * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMalloc(&s.d_status, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(s.d_status, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMallocHost(&s.h_status, sizeof(int));
+  if (e == cudaSuccess) *s.h_status = 0;
   for (int k = 0; k < CONCURRENT_SIDE_MAX && e == cudaSuccess; ++k)
     e = cudaStreamCreateWithFlags(&s.side[k], cudaStreamNonBlocking);
   for (int k = 0; k <= CONCURRENT_SIDE_MAX && e == cudaSuccess; ++k)
@@ -202,6 +222,7 @@ void slot_free(Slot &s) {
   cudaFreeHost(s.h_tmap);
   cudaFree(s.d_counter);
   cudaFree(s.d_status);
+  cudaFreeHost(s.h_status);
   if (s.done) cudaEventDestroy(s.done);
   for (cudaStream_t x : s.side)
     if (x) cudaStreamDestroy(x);
@@ -216,6 +237,13 @@ void retire(cgx_server *sv, int slot) {
   Slot &s = sv->slots[slot];
   const double t = sv->now();
   std::lock_guard<std::mutex> g(sv->mu);
+  if (*s.h_status != CGX_OK) {
+    // a kernel of this launch gave up a bounded wait: its requests' results
+    // are not valid; drain() reports it
+    note_error(sv, set_error(CGX_EDEVICE, "served launch %lld: a device wait ran out (status %d)", s.seq,
+                             *s.h_status));
+    *s.h_status = CGX_OK;
+  }
   for (int r : s.reqs) {
     sv->reqs[r].t_done = t;
     signed char &last = sv->hier_last[sv->ops[sv->reqs[r].op].hier];
@@ -253,7 +281,7 @@ bool launch_batch(cgx_server *sv, int slot) {
       seen[op.hier] = 1;
       if (ntiles + (size_t)op.tiles > s.tile_cap) {
         if (take.empty()) { // larger than a slot (define_op rejects these): drop it
-          sv->error = set_error(CGX_EINVAL, "request larger than a server slot");
+          note_error(sv, set_error(CGX_EINVAL, "request larger than a server slot"));
           sv->reqs[*it].t_done = -1.0;
           sv->completed += 1;
           it = sv->pending.erase(it);
@@ -293,6 +321,7 @@ bool launch_batch(cgx_server *sv, int slot) {
     if (wait_for[k]) e = cudaStreamWaitEvent(s.stream, sv->slots[k].done, 0);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(s.d_tmap, s.h_tmap, ti * sizeof(int2), cudaMemcpyHostToDevice, s.stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.d_status, 0, sizeof(int), s.stream);
   int rc = e == cudaSuccess ? CGX_OK : cuda_error(e, "server slot upload");
   if (rc == CGX_OK && seg[NSEG] > 0) {
     e = cudaMemsetAsync(s.d_counter, 0, NSEG * sizeof(unsigned long long), s.stream);
@@ -302,9 +331,11 @@ bool launch_batch(cgx_server *sv, int slot) {
                                                   &need)
                           : cuda_error(e, "cudaMemsetAsync");
   }
-  if (rc) sv->error = rc;
+  note_error(sv, rc);
+  e = cudaMemcpyAsync(s.h_status, s.d_status, sizeof(int), cudaMemcpyDeviceToHost, s.stream);
+  if (e != cudaSuccess) note_error(sv, cuda_error(e, "server status read-back"));
   e = cudaEventRecord(s.done, s.stream);
-  if (e != cudaSuccess && !sv->error) sv->error = cuda_error(e, "cudaEventRecord");
+  if (e != cudaSuccess) note_error(sv, cuda_error(e, "cudaEventRecord"));
   s.reqs = take;
   s.busy = true;
   s.seq = sv->launches;
@@ -326,12 +357,16 @@ bool launch_plain(cgx_server *sv, Slot &s) {
   }
   const OpTemplate &op = *opp;
   sv->reqs[r].t_launch = sv->now();
+  cudaError_t e = cudaMemsetAsync(s.d_status, 0, sizeof(int), s.stream);
+  if (e != cudaSuccess) note_error(sv, cuda_error(e, "cudaMemsetAsync"));
   for (size_t k = 0; k < op.descs.size(); ++k) {
     int rc = launch_one_pair(op.descs[k], op.ntiles[k], sv->fp, s.d_status, s.stream);
-    if (rc) sv->error = rc;
+    note_error(sv, rc);
   }
-  cudaError_t e = cudaEventRecord(s.done, s.stream);
-  if (e != cudaSuccess && !sv->error) sv->error = cuda_error(e, "cudaEventRecord");
+  e = cudaMemcpyAsync(s.h_status, s.d_status, sizeof(int), cudaMemcpyDeviceToHost, s.stream);
+  if (e != cudaSuccess) note_error(sv, cuda_error(e, "server status read-back"));
+  e = cudaEventRecord(s.done, s.stream);
+  if (e != cudaSuccess) note_error(sv, cuda_error(e, "cudaEventRecord"));
   s.reqs.assign(1, r);
   s.busy = true;
   s.seq = sv->launches;
@@ -598,7 +633,9 @@ int cgx_server_drain(cgx_server *sv) {
   if (!sv->cv.wait_for(g, std::chrono::seconds(600),
                        [&] { return sv->completed.load() >= sv->submitted; }))
     return set_error(CGX_ECUDA, "server drain timed out");
-  return sv->error;
+  std::lock_guard<std::mutex> e(sv->err_mu);
+  if (sv->error) return set_error(sv->error, "%s", sv->error_msg.c_str());
+  return CGX_OK;
 }
 
 int cgx_server_stats(cgx_server *sv, cgx_server_report *rep) {

@@ -308,7 +308,11 @@ int cgx_server_start(cgx_server *s);
 int cgx_server_submit(cgx_server *s, int op_id, int64_t *request_id);
 /* submit op_ids[i] at arrival_s[i] seconds after the call (a load replay) */
 int cgx_server_replay(cgx_server *s, const int *op_ids, const double *arrival_s, int n);
-int cgx_server_drain(cgx_server *s); /* wait until every submitted request is done */
+/* wait until every submitted request is done; returns the worker's first
+ * error, with its message: CGX_EDEVICE when a served launch's kernels gave up
+ * a bounded device wait (each launch's status is read back when its slot
+ * retires), a launch error otherwise */
+int cgx_server_drain(cgx_server *s);
 int cgx_server_stats(cgx_server *s, cgx_server_report *rep);
 int cgx_server_latencies(cgx_server *s, double *out_ms, int64_t n);
 

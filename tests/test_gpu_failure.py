@@ -103,3 +103,43 @@ def test_chain_dependency_wait_runs_out_and_context_recovers(cb):
     torch.cuda.synchronize()
     assert np.array_equal(d0.tensor.cpu().numpy().view(np.uint64), want0.view(np.uint64))
     assert np.array_equal(d1.tensor.cpu().numpy().view(np.uint64), want1.view(np.uint64))
+
+
+def test_served_wait_runs_out_is_reported(cb):
+    """a served launch whose prolongation kernel gives up a bounded wait:
+    the server reads the launch's status back when it retires the slot, and
+    drain() reports CGX_EDEVICE with the worker's message; a new server on
+    the same context then gives what the requests give served alone"""
+    from carpet_b200._lib import lib
+    from carpet_b200.serve import (SERVE_BATCHED, SERVE_PLAIN, Ensemble, Server, ops_for,
+                                   request_key)
+    cb.set_fp_mode(False)
+    sv = Server(mode=SERVE_BATCHED)
+    ens = Ensemble(sv, nhier=2, size_range=(24, 24), seed=5)
+    rng = np.random.default_rng(1)
+    keys = [request_key(ens, m, 1, rng) for m in range(2)]  # boundary prolongations
+    init = ens.snapshot()
+    lib.cgx_debug_skip_tma_plane(1)
+    try:
+        sv.replay(ops_for(ens.ops, keys), [0.0] * len(keys))
+        with pytest.raises(cb.CgxError) as err:
+            sv.drain()
+    finally:
+        lib.cgx_debug_skip_tma_plane(0)
+    assert err.value.code == EDEVICE and "device wait ran out" in str(err.value)
+    sv.close()
+    again, plain = Server(mode=SERVE_BATCHED), Server(mode=SERVE_PLAIN)
+    ops_again, ops_plain = ens.define(again), ens.define(plain)
+    ens.restore(init)
+    again.replay(ops_for(ops_again, keys), [0.0] * len(keys))
+    again.drain()
+    got = [[p.clone() for p in ens.state(m)] for m in range(2)]
+    ens.restore(init)
+    for k in keys:
+        plain.submit(ops_plain[k])
+        plain.drain()
+    for m in range(2):
+        assert all(torch.equal(a.view(torch.int64), b.view(torch.int64))
+                   for a, b in zip(got[m], ens.state(m)))
+    again.close()
+    plain.close()
