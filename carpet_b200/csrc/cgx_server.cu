@@ -74,7 +74,10 @@ struct Request {
 
 struct Slot {
   cudaStream_t stream = nullptr;
-  cudaEvent_t done = nullptr;
+  // done: the launch's kernels have finished (later launches of the same
+  // hierarchies wait for it on the device); fin: its status has also been
+  // read back (the worker retires the slot on it, sleeping if it must)
+  cudaEvent_t done = nullptr, fin = nullptr;
   // the concurrent segment launch: side streams, fork and join events
   cudaStream_t side[CONCURRENT_SIDE_MAX] = {};
   cudaEvent_t ev[CONCURRENT_SIDE_MAX + 1] = {};
@@ -158,7 +161,8 @@ void note_error(cgx_server *sv, int rc) {
 int slot_init(Slot &s, size_t tile_cap) {
   cudaError_t e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
   // blocking sync: a worker that waits on it sleeps instead of spinning
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming | cudaEventBlockingSync);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.fin, cudaEventDisableTiming | cudaEventBlockingSync);
   if (e == cudaSuccess) e = cudaMalloc(&s.d_tmap, tile_cap * sizeof(int2));
   if (e == cudaSuccess) e = cudaMallocHost(&s.h_tmap, tile_cap * sizeof(int2));
   // claim counters and exit counts (cgx_kernels.cuh, claims_done)
@@ -224,6 +228,7 @@ void slot_free(Slot &s) {
   cudaFree(s.d_status);
   cudaFreeHost(s.h_status);
   if (s.done) cudaEventDestroy(s.done);
+  if (s.fin) cudaEventDestroy(s.fin);
   for (cudaStream_t x : s.side)
     if (x) cudaStreamDestroy(x);
   for (cudaEvent_t x : s.ev)
@@ -316,25 +321,26 @@ bool launch_batch(cgx_server *sv, int slot) {
   seg[NSEG] = (long long)ti;
   const double t = sv->now();
   for (int r : take) sv->reqs[r].t_launch = t;
-  cudaError_t e = cudaSuccess;
+  // the slot's own uploads and resets first, then the waits for the slots
+  // that hold these hierarchies' previous requests: only the kernels sit
+  // behind those on the device
+  cudaError_t e = cudaMemcpyAsync(s.d_tmap, s.h_tmap, ti * sizeof(int2), cudaMemcpyHostToDevice, s.stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.d_status, 0, sizeof(int), s.stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.d_counter, 0, NSEG * sizeof(unsigned long long), s.stream);
   for (int k = 0; k < SERVER_SLOTS && e == cudaSuccess; ++k)
     if (wait_for[k]) e = cudaStreamWaitEvent(s.stream, sv->slots[k].done, 0);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(s.d_tmap, s.h_tmap, ti * sizeof(int2), cudaMemcpyHostToDevice, s.stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(s.d_status, 0, sizeof(int), s.stream);
   int rc = e == cudaSuccess ? CGX_OK : cuda_error(e, "server slot upload");
   if (rc == CGX_OK && seg[NSEG] > 0) {
-    e = cudaMemsetAsync(s.d_counter, 0, NSEG * sizeof(unsigned long long), s.stream);
     int need = 0;
-    rc = e == cudaSuccess ? launch_map_concurrent(sv->fp, pdescs, pmaps, s.d_tmap, seg, sv->tma_cfg, s.d_counter,
-                                                  s.d_status, s.stream, s.side, s.ev, CONCURRENT_SIDE_MAX,
-                                                  &need)
-                          : cuda_error(e, "cudaMemsetAsync");
+    rc = launch_map_concurrent(sv->fp, pdescs, pmaps, s.d_tmap, seg, sv->tma_cfg, s.d_counter, s.d_status,
+                               s.stream, s.side, s.ev, CONCURRENT_SIDE_MAX, &need);
   }
   note_error(sv, rc);
+  e = cudaEventRecord(s.done, s.stream);
+  if (e != cudaSuccess) note_error(sv, cuda_error(e, "cudaEventRecord"));
   e = cudaMemcpyAsync(s.h_status, s.d_status, sizeof(int), cudaMemcpyDeviceToHost, s.stream);
   if (e != cudaSuccess) note_error(sv, cuda_error(e, "server status read-back"));
-  e = cudaEventRecord(s.done, s.stream);
+  e = cudaEventRecord(s.fin, s.stream);
   if (e != cudaSuccess) note_error(sv, cuda_error(e, "cudaEventRecord"));
   s.reqs = take;
   s.busy = true;
@@ -365,7 +371,7 @@ bool launch_plain(cgx_server *sv, Slot &s) {
   }
   e = cudaMemcpyAsync(s.h_status, s.d_status, sizeof(int), cudaMemcpyDeviceToHost, s.stream);
   if (e != cudaSuccess) note_error(sv, cuda_error(e, "server status read-back"));
-  e = cudaEventRecord(s.done, s.stream);
+  e = cudaEventRecord(s.fin, s.stream);
   if (e != cudaSuccess) note_error(sv, cuda_error(e, "cudaEventRecord"));
   s.reqs.assign(1, r);
   s.busy = true;
@@ -381,7 +387,7 @@ void worker_loop(cgx_server *sv) {
     bool progress = false;
     for (int i = 0; i < nslots; ++i) {
       Slot &s = sv->slots[i];
-      if (s.busy && cudaEventQuery(s.done) == cudaSuccess) {
+      if (s.busy && cudaEventQuery(s.fin) == cudaSuccess) {
         retire(sv, i);
         progress = true;
       }
@@ -410,7 +416,7 @@ void worker_loop(cgx_server *sv) {
       if (all_busy) {
         // nothing can launch before a slot frees: sleep on the oldest
         // slot's blocking-sync event (no core spins meanwhile)
-        cudaEventSynchronize(sv->slots[oldest].done);
+        cudaEventSynchronize(sv->slots[oldest].fin);
       } else {
         // a free slot and nothing pending: wake for a new request or,
         // after a short while, to poll the busy slot again
