@@ -173,3 +173,64 @@ def test_admission_while_serving(cgx):
     assert _equal(got, ens.state(m))
     sv.close()
     plain.close()
+
+
+def test_each_request_type_matches_the_oracle(cgx):
+    """every operation of a hierarchy -- the sync of each level, the
+    boundary prolongation of each refined level (order 5, 3-timelevel time
+    interpolation), the restriction into each coarser level and the regrid
+    fill of the moved finest level -- served through the batched server
+    gives, bit for bit, what the oracle gives for the same box-pairs on
+    host copies of the same arrays"""
+    from carpet_b200.moving import old2new
+    from carpet_b200.serve import SERVE_BATCHED, Ensemble, Server
+    from oracle.binding import OP_LAGRANGE, VERTEX, Port
+    cgx.set_fp_mode(False)
+    port = Port()
+    sv = Server(mode=SERVE_BATCHED)
+    ens = Ensemble(sv, nhier=2, size_range=(24, 32), seed=17, regrid=True)
+    m = 1
+    mem = ens.members[m]
+    h, st, L = mem.hier, mem.storage, len(mem.hier.levels)
+    dtc = 1.0 / 64
+    times3 = [0.0, -dtc, -2 * dtc]
+    kinds = set()
+    for key in sorted(k for k in ens.ops if k[0] == m):
+        _, kind, l = key
+        calls = []  # (dst, srcs, dstbox, srcbox, times, time, order_space, order_time)
+        for g in range(st.ngf):
+            if kind == "sync":
+                a = st.data[l][0][g]
+                calls += [(a[p.dst_comp], [a[p.src_comp]], p.dstbox, p.srcbox, [0.0], 0.0, 1, 0)
+                          for p in h.sync[l]]
+            elif kind == "prolong":
+                calls += [(st.data[l][0][g][p.dst_comp], [st.data[l - 1][t][g][p.src_comp] for t in range(3)],
+                           p.dstbox, p.srcbox, times3, -dtc / 2, 5, 2) for p in h.prolong[l]]
+            elif kind == "restrict":
+                calls += [(st.data[l][0][g][p.dst_comp], [st.data[l + 1][0][g][p.src_comp]], p.dstbox,
+                           p.srcbox, [0.0], 0.0, 5, 0) for p in h.restrict[l + 1]]
+        if kind == "regrid":
+            copies, prols = old2new(h, mem.moved, l)
+            for tl in range(st.ntl):
+                dst = mem.moved_storage.data[l][tl]
+                for g in range(st.ngf):
+                    calls += [(dst[g][p.dst_comp], [st.data[l][tl][g][p.src_comp]], p.dstbox, p.srcbox,
+                               [0.0], 0.0, 1, 0) for p in copies]
+                    calls += [(dst[g][p.dst_comp], [st.data[l - 1][tl][g][p.src_comp]], p.dstbox,
+                               p.srcbox, [0.0], 0.0, 5, 0) for p in prols]
+        assert calls, key
+        kinds.add(kind)
+        datas = {}
+        for dst, srcs, *_ in calls:
+            for d in [dst] + srcs:
+                datas[id(d)] = d
+        host = {i: d.tensor.cpu().numpy().copy() for i, d in datas.items()}
+        for dst, srcs, dbox, sbox, tms, t, osp, ot in calls:
+            port.transfer(OP_LAGRANGE, VERTEX, host[id(dst)], list(dst.extent), [host[id(s)] for s in srcs],
+                          list(srcs[0].extent), tms, list(dbox), list(sbox), t, osp, ot)
+        sv.submit(ens.ops[key])
+        sv.drain()
+        for i, d in datas.items():
+            assert np.array_equal(d.tensor.cpu().numpy().view(np.uint64), host[i].view(np.uint64)), key
+    assert kinds == {"sync", "prolong", "restrict", "regrid"}
+    sv.close()
