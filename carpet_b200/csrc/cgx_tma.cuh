@@ -289,9 +289,11 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
     for (int p = 0; p < PD; ++p)
       if (p < nplanes) issue(p);
   }
-  // Iteration i: stage plane i + PD; wait for plane i and run its x pass
-  // (DX: i < nplanes); run the y/z pass of plane i - 1 (DY: i >= 1).  The
-  // barrier also reduces the waits' failures (__syncthreads_or).  With
+  // Iteration i: stage plane i + PD; run the y/z pass of plane i - 1 (DY:
+  // i >= 1), on x-pass rows finished before the previous iteration's
+  // barrier, which gives the copy of plane i time to land; wait for plane i
+  // and run its x pass (DX: i < nplanes); then the barrier, which also
+  // reduces the waits' failures (__syncthreads_or).  With
   // SPLIT (one timelevel: a short loop body) the whole groups of Q
   // iterations run without per-iteration checks and a second unrolled copy
   // handles the last ones.
@@ -300,30 +302,27 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
     constexpr bool X = decltype(DX)::value, Y = decltype(DY)::value;
     if (!ok) return; // uniform: a wait gave up
     if (tid == 0 && i + PD < nplanes) issue(i + PD);
+    if (Y) yzpass(Ut, i - 1, xrows + ((i - 1) & 1) * S::xbuf);
     const unsigned g = g0 + (unsigned)i;
     const int fail = X ? !mbar_wait_bounded(&ring.bars[g % NB], (g / NB) & 1) : 0;
+    if (X && !fail) xpass((int)(g % NB), xrows + (i & 1) * S::xbuf);
     if (__syncthreads_or(fail)) {
       if (tid == 0) *ring.abort = 1;
       ok = false;
-      return;
     }
-    if (X) xpass((int)(g % NB), xrows + (i & 1) * S::xbuf);
-    if (Y) yzpass(Ut, i - 1, xrows + ((i - 1) & 1) * S::xbuf);
   };
   // the same iteration with run-time checks, one unrolled copy: the loop of
   // the multi-timelevel variants, whose long bodies make a second unrolled
   // copy (and its register allocation) cost more than the checks
   auto iteration_rt = [&](auto Ut, int i) {
     if (tid == 0 && i + PD < nplanes) issue(i + PD);
-    const unsigned g = g0 + (unsigned)i;
-    if (i < nplanes && !mbar_wait_bounded(&ring.bars[g % NB], (g / NB) & 1)) *ring.abort = 1;
-    __syncthreads();
-    if (*ring.abort) {
-      ok = false;
-      return;
-    }
-    if (i < nplanes) xpass((int)(g % NB), xrows + (i & 1) * S::xbuf);
     if (i >= 1) yzpass(Ut, i - 1, xrows + ((i - 1) & 1) * S::xbuf);
+    const unsigned g = g0 + (unsigned)i;
+    const bool landed = i < nplanes && mbar_wait_bounded(&ring.bars[g % NB], (g / NB) & 1);
+    if (landed) xpass((int)(g % NB), xrows + (i & 1) * S::xbuf);
+    else if (i < nplanes) *ring.abort = 1;
+    __syncthreads();
+    if (*ring.abort) ok = false;
   };
   using T_ = std::true_type;
   using F_ = std::false_type;
