@@ -289,11 +289,14 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
     for (int p = 0; p < PD; ++p)
       if (p < nplanes) issue(p);
   }
-  // Iteration i: stage plane i + PD; run the y/z pass of plane i - 1 (DY:
-  // i >= 1), on x-pass rows finished before the previous iteration's
-  // barrier, which gives the copy of plane i time to land; wait for plane i
-  // and run its x pass (DX: i < nplanes); then the barrier, which also
-  // reduces the waits' failures (__syncthreads_or).  With
+  // One-timelevel iteration i: stage plane i + PD; wait for plane i (the
+  // barrier also reduces the waits' failures, __syncthreads_or), run its x
+  // pass (DX: i < nplanes) and the y/z pass of plane i - 1 (DY: i >= 1).
+  // Multi-timelevel iteration i (iteration_rt): stage plane i + PD, run the
+  // y/z pass of plane i - 1 first -- on x-pass rows finished before the
+  // previous iteration's barrier -- which gives the copies of plane i a
+  // long pass's time to land, then wait for plane i, run its x pass, and
+  // end with the barrier.  With
   // SPLIT (one timelevel: a short loop body) the whole groups of Q
   // iterations run without per-iteration checks and a second unrolled copy
   // handles the last ones.
@@ -302,14 +305,15 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
     constexpr bool X = decltype(DX)::value, Y = decltype(DY)::value;
     if (!ok) return; // uniform: a wait gave up
     if (tid == 0 && i + PD < nplanes) issue(i + PD);
-    if (Y) yzpass(Ut, i - 1, xrows + ((i - 1) & 1) * S::xbuf);
     const unsigned g = g0 + (unsigned)i;
     const int fail = X ? !mbar_wait_bounded(&ring.bars[g % NB], (g / NB) & 1) : 0;
-    if (X && !fail) xpass((int)(g % NB), xrows + (i & 1) * S::xbuf);
     if (__syncthreads_or(fail)) {
       if (tid == 0) *ring.abort = 1;
       ok = false;
+      return;
     }
+    if (X) xpass((int)(g % NB), xrows + (i & 1) * S::xbuf);
+    if (Y) yzpass(Ut, i - 1, xrows + ((i - 1) & 1) * S::xbuf);
   };
   // the same iteration with run-time checks, one unrolled copy: the loop of
   // the multi-timelevel variants, whose long bodies make a second unrolled
