@@ -545,6 +545,7 @@ def main():
         replicas.init("nccl", timeout_s=120)
     import carpet_b200 as cb
     from carpet_b200.amr import BergerOliger, Storage
+    from carpet_b200.bo import fp64_ops, phase_pairs
     from carpet_b200.hierarchy import nested
 
     cb.set_fp_mode(args.fp == "fma")
@@ -649,16 +650,27 @@ def main():
         b_.record(stream)
     stream.synchronize()
     phases = {}
+    fp64_of = {}
     for (a, b_), (k, b) in zip(evs, launches):
         name = PHASE_KERNELS[(k[0], k[3])]
         e = phases.setdefault(name, {"launches": 0, "ms": 0.0, "bytes": 0})
         e["launches"] += 1
         e["ms"] += a.elapsed_time(b_)
         e["bytes"] += b.stats()["bytes"]
+        if k not in fp64_of:
+            pairs, _, _ = phase_pairs(h, k)
+            fp64_of[k] = args.ngf * sum(fp64_ops(k[0], k[3], q.dstbox, q.srcbox, 5) for q in pairs)
+        e["fp64_ops"] = e.get("fp64_ops", 0) + fp64_of[k]
     tot_ms = sum(e["ms"] for e in phases.values())
+    # FP64 peak: 64 double-precision lanes per SM (B200) at the maximum SM clock
+    sm_count = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    fp64_peak = 64 * sm_count * (clk.smax or 1965.0) * 1e6 / 1e12  # T ops/s
     for e in phases.values():
         e["gbs"] = round(e["bytes"] / (e["ms"] * 1e-3) / 1e9, 1)
         e["share"] = round(e["ms"] / tot_ms, 3)
+        if e["fp64_ops"]:
+            e["fp64_tops"] = round(e["fp64_ops"] / (e["ms"] * 1e-3) / 1e12, 3)
+            e["fp64_frac"] = round(e["fp64_tops"] / fp64_peak, 4)
         e["ms"] = round(e["ms"], 3)
     dom = max(phases, key=lambda n: phases[n]["ms"])
     peaks = {}
@@ -847,7 +859,13 @@ def main():
                          "kernel": dom, "algorithmic_bytes_per_launch": int(bytes_per_launch),
                          "launch": f"one launch over all {args.ngf} grid functions, timed alone",
                          "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks
-                         else "fallback 6650 GB/s"},
+                         else "fallback 6650 GB/s",
+                         "fp64": None if not phases[dom].get("fp64_ops") else {
+                             "achieved": phases[dom]["fp64_tops"], "peak": round(fp64_peak, 2),
+                             "unit": "T ops/s", "frac": phases[dom]["fp64_frac"],
+                             "ops_per_launch": int(phases[dom]["fp64_ops"] / phases[dom]["launches"]),
+                             "ops": "multiplies and adds of the separable bit-exact evaluation",
+                             "peak_source": "nominal: 64 FP64 lanes per SM x SMs x max SM clock"}},
             "phases": phases, "parity": parity,
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(), "served": serve,
             "batched_uneven": batched_uneven, "moving_boxes": moving_boxes,

@@ -96,6 +96,36 @@ def stencil_points(reg, srcbbox, order: int = 5) -> int:
     return n
 
 
+def fp64_ops(kind: str, ntl: int, reg, srcbbox, order: int = 5) -> int:
+    """the double-precision operations a bit-exact, separable evaluation of
+    one vertex-centred prolongation box-pair cannot avoid, in the exact mode
+    (every product and every sum its own rounding, as prolongate_3d_rf2.cc
+    computes them without contraction): a (order + 1)-tap sum costs order + 1
+    multiplies and order adds; the x pass evaluates every odd fine x on every
+    coarse (y, z) the region's windows touch, the y pass every odd fine y on
+    every coarse z, the z pass every odd fine z; even fine points are copies.
+    Time interpolation adds ntl multiplies and ntl - 1 adds per fine point.
+    Copies and injection have no arithmetic (0)."""
+    if kind != "prolong":
+        return 0
+    lo1, hi1 = -(order // 2), order // 2 + 1
+    m, odd, coarse = [], [], []
+    for d in range(3):
+        soff = (reg[d] - srcbbox[d]) // reg[6 + d]
+        n = (reg[3 + d] - reg[d]) // reg[6 + d] + 1
+        m.append(n)
+        odd.append(sum(1 for i in range(n) if (soff + i) & 1))
+        cs = [soff + i for i in range(min(2, n))] + [soff + i for i in range(max(0, n - 2), n)]
+        lo = min((s >> 1) + (lo1 if s & 1 else 0) for s in cs)
+        hi = max((s >> 1) + (hi1 if s & 1 else 0) for s in cs)
+        coarse.append(hi - lo + 1)
+    taps = (odd[0] * coarse[1] * coarse[2] + m[0] * odd[1] * coarse[2] + m[0] * m[1] * odd[2])
+    ops = ntl * taps * (2 * (order + 1) - 1)
+    if ntl > 1:
+        ops += (2 * ntl - 1) * m[0] * m[1] * m[2]
+    return ops
+
+
 def algorithmic_bytes(kind: str, ntl: int, dstbox, srcbox, order: int = 5) -> int:
     """the algorithmic bytes of one box-pair: copy 16 B per destination
     point, injection 16 B per coarse point, prolongation 8 B per fine point
