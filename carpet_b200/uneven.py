@@ -138,3 +138,56 @@ def uneven_batch(pairs: List[UnevenPair]) -> Batch:
         sp = p.spec
         b.add(p.dst, [p.src], [0.0], sp.reg, sp.srcbbox, 0.0, sp.order, 0, op=sp.op, cent=sp.cent)
     return b
+
+
+def main(argv=None):
+    """``python -m carpet_b200.uneven``: the 256-pair uneven batch alone
+    (autotuned or pinned tiles, one graph replay per step), printed as one
+    JSON line -- the workload the profiles of the mixed batch are taken on"""
+    import argparse
+    import json
+
+    from . import transfer
+    from .transfer import Graph
+
+    p = argparse.ArgumentParser(prog="python -m carpet_b200.uneven")
+    p.add_argument("--pairs", type=int, default=256)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--tile-config", type=int, default=None,
+                   help="pin every prolongation variant to this configuration instead of tuning")
+    p.add_argument("--fp", default="exact", choices=["exact", "fma"])
+    a = p.parse_args(argv)
+    transfer.set_fp_mode(a.fp == "fma")
+    pairs = uneven_pairs(uneven_specs(seed=3, npairs=a.pairs, ext=(16, 96)), seed=4)
+    b = uneven_batch(pairs)
+    st = b.stats()
+    if a.tile_config is None:
+        configs = sorted(set(b.autotune(reps=3).values()))
+    else:
+        b.set_config(a.tile_config)
+        b.upload()
+        configs = [a.tile_config]
+    s = torch.cuda.Stream()
+    g = Graph()
+    with g.capture(s):
+        b.launch(s)
+    for _ in range(a.warmup):
+        g.launch(s)
+    s.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(a.steps):
+        g.launch(s)
+    e1.record(s)
+    s.synchronize()
+    b.check(s)
+    ms = e0.elapsed_time(e1) / a.steps
+    print(json.dumps({"pairs": st["pairs"], "fine_points": st["points"], "bytes": st["bytes"],
+                      "ms": round(ms, 4), "gbs": round(st["bytes"] / (ms * 1e-3) / 1e9, 1),
+                      "tile_configs": configs, "fp_mode": a.fp}))
+    del g
+
+
+if __name__ == "__main__":
+    main()
