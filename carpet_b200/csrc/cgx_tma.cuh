@@ -253,7 +253,9 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
 #pragma unroll
       for (int q = 0; q < Q; ++q) yq[t][h][q] = 0.0;
 
-  auto yzpass = [&](auto Ut, int p, const double *__restrict__ xr) {
+  // o0: this thread's store address in fine plane 2 * (cz0 + p - HI), carried
+  // by the multi-timelevel loop (the one-timelevel loop computes it here)
+  auto yzpass = [&](auto Ut, int p, const double *__restrict__ xr, double *o0) {
     constexpr int U = decltype(Ut)::value;
     if (!wact) return; // warp-uniform
 #pragma unroll
@@ -268,7 +270,9 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
     for (int zp = 0; zp < 2; ++zp) {
       const int zs = 2 * cb + zp;
       const bool zok = zs >= sz0 && zs < sz0 + nfz; // uniform
-      double *o = obase + (long long)zs * dsz;
+      double *o;
+      if constexpr (SPLIT) o = obase + (long long)zs * dsz;
+      else o = zp ? o0 + dsz : o0;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         double v[NTL];
@@ -313,20 +317,35 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
       return;
     }
     if (X) xpass((int)(g % NB), xrows + (i & 1) * S::xbuf);
-    if (Y) yzpass(Ut, i - 1, xrows + ((i - 1) & 1) * S::xbuf);
+    if (Y) yzpass(Ut, i - 1, xrows + ((i - 1) & 1) * S::xbuf, nullptr);
   };
   // the same iteration with run-time checks, one unrolled copy: the loop of
   // the multi-timelevel variants, whose long bodies make a second unrolled
-  // copy (and its register allocation) cost more than the checks
+  // copy (and its register allocation) cost more than the checks.  Its
+  // plane-dependent addresses are carried from one iteration to the next
+  // rather than recomputed: the ring slot and phase of plane i (slot
+  // (g0 + i) % NB, phase (g0 + i) / NB) and the store address of the y/z
+  // pass's plane i - 1.
+  int rslot = (int)(g0 % NB);
+  unsigned rpar = (g0 / NB) & 1;
+  double *oz = obase + (long long)(2 * (cz0 - HI)) * dsz;
+  const long long dz2 = 2 * dsz;
   auto iteration_rt = [&](auto Ut, int i) {
     if (tid == 0 && i + PD < nplanes) issue(i + PD);
-    if (i >= 1) yzpass(Ut, i - 1, xrows + ((i - 1) & 1) * S::xbuf);
-    const unsigned g = g0 + (unsigned)i;
-    const bool landed = i < nplanes && mbar_wait_bounded(&ring.bars[g % NB], (g / NB) & 1);
-    if (landed) xpass((int)(g % NB), xrows + (i & 1) * S::xbuf);
-    else if (i < nplanes) *ring.abort = 1;
-    __syncthreads();
-    if (*ring.abort) ok = false;
+    if (i >= 1) {
+      yzpass(Ut, i - 1, xrows + ((i - 1) & 1) * S::xbuf, oz);
+      oz += dz2;
+    }
+    const bool landed = i < nplanes && mbar_wait_bounded(&ring.bars[rslot], rpar);
+    if (landed) xpass(rslot, xrows + (i & 1) * S::xbuf);
+    if (++rslot == NB) {
+      rslot = 0;
+      rpar ^= 1u;
+    }
+    if (__syncthreads_or(i < nplanes && !landed)) { // a wait gave up
+      if (tid == 0) *ring.abort = 1;
+      ok = false;
+    }
   };
   using T_ = std::true_type;
   using F_ = std::false_type;
