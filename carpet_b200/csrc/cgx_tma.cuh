@@ -181,11 +181,17 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
 
   int issued = 0; // planes staged so far (elected thread)
   const int skip = g0 == 0 ? ring.skip : -1;
-  auto issue = [&](int p) { // elected thread: stage plane p
+  int islot = (int)(g0 % NB); // multi-timelevel: ring slot of the next plane staged
+  auto issue = [&](int p) {   // elected thread: stage plane p (p = 0, 1, ...)
     issued = p + 1;
+    int slot;
+    if constexpr (SPLIT) {
+      slot = (int)((g0 + (unsigned)p) % NB);
+    } else {
+      slot = islot;
+      if (++islot == NB) islot = 0;
+    }
     if (p == skip) return; // failure injection: this plane never lands
-    const unsigned g = g0 + (unsigned)p;
-    const int slot = (int)(g % NB);
     mbar_expect_tx(&ring.bars[slot], (unsigned)(NTL * BX * BY * 8));
 #pragma unroll
     for (int t = 0; t < NTL; ++t)
@@ -211,11 +217,12 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
   }
   auto xpass = [&](int slot, double *__restrict__ xr) {
     const double *__restrict__ cs = coarse + slot * NTL * G::TLS - LO;
-    // with SPLIT every thread runs all IT items (the ones past the plane's
-    // count read the slot's first points and write the spare row)
+    // every thread runs its items of all rounds but, without SPLIT, the last
+    // one when the tile has no item there (items past the plane's count read
+    // the slot's first points and write the spare row)
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
-      if (SPLIT || k * NT < count) { // uniform
+      if (SPLIT || k < IT - 1 || k * NT < count) { // uniform
         const double *row = cs + xsrc[k];
         auto get = [&](int m) { return row[m]; };
         const double xe = F::template first<FMA>(0, get);
@@ -324,20 +331,24 @@ __device__ bool prolong_tile_tma(const Desc &d, const CUtensorMap *__restrict__ 
   // copy (and its register allocation) cost more than the checks.  Its
   // plane-dependent addresses are carried from one iteration to the next
   // rather than recomputed: the ring slot and phase of plane i (slot
-  // (g0 + i) % NB, phase (g0 + i) / NB) and the store address of the y/z
-  // pass's plane i - 1.
+  // (g0 + i) % NB, phase (g0 + i) / NB), the x-pass rows of planes i and
+  // i - 1, and the store address of the y/z pass's plane i - 1.
   int rslot = (int)(g0 % NB);
   unsigned rpar = (g0 / NB) & 1;
   double *oz = obase + (long long)(2 * (cz0 - HI)) * dsz;
   const long long dz2 = 2 * dsz;
+  double *xcur = xrows, *xprev = xrows + S::xbuf; // x-pass rows of planes i, i - 1
   auto iteration_rt = [&](auto Ut, int i) {
     if (tid == 0 && i + PD < nplanes) issue(i + PD);
     if (i >= 1) {
-      yzpass(Ut, i - 1, xrows + ((i - 1) & 1) * S::xbuf, oz);
+      yzpass(Ut, i - 1, xprev, oz);
       oz += dz2;
     }
     const bool landed = i < nplanes && mbar_wait_bounded(&ring.bars[rslot], rpar);
-    if (landed) xpass(rslot, xrows + (i & 1) * S::xbuf);
+    if (landed) xpass(rslot, xcur);
+    double *const xt = xcur;
+    xcur = xprev;
+    xprev = xt;
     if (++rslot == NB) {
       rslot = 0;
       rpar ^= 1u;
